@@ -1,0 +1,175 @@
+/*
+ * tapas_b200.h - C ABI of libtapas_b200.so, the sm_100a (B200) implementation
+ * of the Tapas N-body evaluation path (octree build, upward pass, dual-tree
+ * traversal with M2L + P2P, downward pass) for the ExaFMM Laplace
+ * spherical-harmonics kernels and the Barnes-Hut monopole sample.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: 0 (TAPAS_B200_OK) or a negative
+ *    tapas_b200_status.  Nothing calls exit() or abort(); the reference's
+ *    CUDA_SAFE_CALL/assert error paths (cpp/include/tapas/common.h:278-287,
+ *    vectormap_cuda.h:70-80) become status codes plus tapas_b200_last_error().
+ *  - Plain pointers and sizes only.  `mem` arguments say whether a pointer is
+ *    host memory (TAPAS_B200_HOST) or device memory (TAPAS_B200_DEVICE) on
+ *    the context's GPU.
+ *  - All GPU work of a context is issued on its stream (tapas_b200_set_stream);
+ *    calls that return host data synchronise that stream.
+ *  - Bodies are structure-of-arrays FP64 x, y, z, q.  Results are four values
+ *    per body, (pot, ax, ay, az) per unit charge, exactly what the reference's
+ *    TRG holds after L2P (ExaFMM kvec4, ex/LaplaceSphericalCPU_tapas.h:275-307).
+ *
+ * Reference paths below are relative to the reference project;
+ * "ex/" = sample/exafmm-dev-13274dd4ac68/examples/.
+ */
+#ifndef TAPAS_B200_H_
+#define TAPAS_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tapas_b200_ctx tapas_b200_ctx;
+
+typedef enum {
+  TAPAS_B200_OK = 0,
+  TAPAS_B200_ERR_ARG = -1,         /* invalid argument                         */
+  TAPAS_B200_ERR_CUDA = -2,        /* CUDA runtime error (see last_error)      */
+  TAPAS_B200_ERR_NOMEM = -3,       /* device or host allocation failed         */
+  TAPAS_B200_ERR_STATE = -4,       /* call out of order (e.g. upward before partition) */
+  TAPAS_B200_ERR_CAPACITY = -5,    /* a device work queue hit its bound        */
+  TAPAS_B200_ERR_UNSUPPORTED = -6, /* e.g. mutual=1, expansion order outside 2..16 */
+  TAPAS_B200_ERR_TIMEOUT = -7      /* a bounded device wait gave up            */
+} tapas_b200_status;
+
+enum { TAPAS_B200_HOST = 0, TAPAS_B200_DEVICE = 1 };
+
+/* Arithmetic of the expansion and near-field kernels. */
+enum {
+  TAPAS_B200_FP64 = 0,  /* plain FP64 everywhere (the reference's FP64 build)          */
+  TAPAS_B200_MIXED = 1  /* FP32 compensated P2P, split-precision tensor-core M2L,
+                           FP64 M2M/L2L at tree levels <= 3 and FP64 final sums        */
+};
+
+/* Output order of per-body results. */
+enum {
+  TAPAS_B200_ORDER_SORTED = 0,   /* Morton order, as CopyBackResult leaves them
+                                    (ex/tapas_exafmm.cxx:388-398)                     */
+  TAPAS_B200_ORDER_ORIGINAL = 1  /* the caller's input order                          */
+};
+
+typedef struct {
+  int64_t n_bodies;
+  int64_t n_cells;
+  int64_t n_leaves;
+  int32_t max_depth;
+  int32_t ncrit;
+  double box_lo, box_hi; /* the cube [lo,hi]^3 the keys are quantised in */
+} tapas_b200_tree_stats;
+
+typedef struct {
+  int64_t n_m2l;               /* M2L translations (cell pairs)                     */
+  int64_t n_p2p;               /* P2P leaf pairs with both leaves non-empty        */
+  uint64_t n_p2p_interactions; /* sum over leaf pairs of nb_i * nb_j              */
+  int32_t traverse_iterations;
+} tapas_b200_list_stats;
+
+/* Phase timings of the last calls, milliseconds, measured with CUDA events on
+ * the context stream when profiling is on (tapas_b200_set_profiling). */
+typedef struct {
+  double upload, bbox_keys, sort, tree, upward, p2m, m2m, traverse, list_sort, m2l, p2p,
+      downward, l2l, l2p, download;
+} tapas_b200_timings;
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Replaces Vectormap_CUDA_Base::Setup (cpp/include/tapas/vectormap_cuda.h:337-395):
+ * binds the context to `device`, creates its stream, checks it is sm_100. */
+int tapas_b200_ctx_create(int device, tapas_b200_ctx **out);
+/* Replaces Vectormap_CUDA_Base::Release (vectormap_cuda.h:397-404). */
+int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx);
+/* Use `stream` (a cudaStream_t) for all later work; NULL restores the context's own. */
+int tapas_b200_set_stream(tapas_b200_ctx *ctx, void *stream);
+int tapas_b200_set_profiling(tapas_b200_ctx *ctx, int on);
+int tapas_b200_get_timings(tapas_b200_ctx *ctx, tapas_b200_timings *out);
+/* Message of the last failing call on this context ("" if none). Thread-local
+ * fallback when ctx is NULL (e.g. ctx_create failure). */
+const char *tapas_b200_last_error(const tapas_b200_ctx *ctx);
+/* Number of kernel launches issued by this context since the last reset. */
+int64_t tapas_b200_kernel_launches(tapas_b200_ctx *ctx, int reset);
+
+/* ---- tree ---------------------------------------------------------------- */
+
+/* Replaces tapas::Tapas<TSP>::Partition (cpp/include/tapas/hot.h:1349-1352) ->
+ * Partitioner::Partition (hot.h:1241-1284) -> SamplingOctree::Build
+ * (hot/buildtree.h:329-367): bounding cube, Morton keys (buildtree.h:505-539),
+ * key sort (common.h:249-273), cell tree (buildtree.h:388-459; a cell is a
+ * leaf iff it holds <= ncrit bodies, non-leaves always have 8 children).
+ * Single rank: the MPI sampling / exchange steps reduce to the identity. */
+int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, const double *z,
+                         const double *q, int64_t n, int ncrit, int mem);
+int tapas_b200_tree_info(tapas_b200_ctx *ctx, tapas_b200_tree_stats *out);
+/* Cells in breadth-first (level) order; any output may be NULL.  bbeg/nb are
+ * the body range in sorted order; child0 = index of the first of 8 children
+ * (-1 for leaves); center3/width3 = 3 doubles per cell. Host memory. */
+int tapas_b200_get_cells(tapas_b200_ctx *ctx, uint64_t *key, int32_t *leaf, int32_t *nb,
+                         int32_t *bbeg, int32_t *parent, int32_t *child0, double *center3,
+                         double *width3);
+/* Sorted bodies: original index and Morton key per sorted position. Host memory. */
+int tapas_b200_get_sorted(tapas_b200_ctx *ctx, int64_t *orig_index, uint64_t *keys);
+
+/* ---- evaluation ---------------------------------------------------------- */
+
+/* Replaces TapasFMM::Map(FMM_Upward(), *root, theta) (ex/tapas_exafmm.cxx:586):
+ * FMM_Upward (:87-122) -> P2M (ex/LaplaceSphericalCPU_tapas.h:138-163) per leaf
+ * and M2M (:165-206) per non-leaf, children before parents.  P in 2..16. */
+int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision);
+
+/* Replaces TapasFMM::Map(FMM_DTT(), tapas::Product(*root, *root), mutual,
+ * nspawn, theta) (ex/tapas_exafmm.cxx:606) together with the GPU mapper's
+ * body-pair offload (hot/mapper.h:453-690, vectormap_cuda.h:826-1005):
+ * builds the M2L and P2P lists with the FMM_DTT acceptance test and split
+ * rule (:209-286) and evaluates M2L (LaplaceSphericalCPU_tapas.h:208-273) and
+ * P2P (LaplaceP2PCPU_tapas.h:23-74).  mutual must be 0, as in the reference's
+ * CUDA build (ex/tapas_exafmm.cxx:507-515). */
+int tapas_b200_traverse(tapas_b200_ctx *ctx, double theta, int mutual, int precision);
+/* The same, in steps: list construction only, then each list. */
+int tapas_b200_build_lists(tapas_b200_ctx *ctx, double theta, int mutual);
+int tapas_b200_list_info(tapas_b200_ctx *ctx, tapas_b200_list_stats *out);
+/* Copies the lists (cell indices in the get_cells order, sorted by target then
+ * source) to host memory; arrays must hold list_info counts. */
+int tapas_b200_get_lists(tapas_b200_ctx *ctx, int32_t *m2l_tgt, int32_t *m2l_src,
+                         int32_t *p2p_tgt, int32_t *p2p_src);
+int tapas_b200_m2l(tapas_b200_ctx *ctx, int precision);
+int tapas_b200_p2p(tapas_b200_ctx *ctx, int precision);
+
+/* Replaces TapasFMM::Map(FMM_Downward(), *root) (ex/tapas_exafmm.cxx:627):
+ * L2L (LaplaceSphericalCPU_tapas.h:309-345) parent before child, then L2P
+ * (:275-307) for every non-empty leaf. */
+int tapas_b200_downward(tapas_b200_ctx *ctx, int precision);
+
+/* Multipole / local expansions, ncells x P(P+1)/2 complex FP64 values as
+ * interleaved (re, im), cells in get_cells order.  Host memory; either may be NULL. */
+int tapas_b200_get_expansions(tapas_b200_ctx *ctx, double *M, double *L);
+
+/* Replaces CopyBackResult (ex/tapas_exafmm.cxx:388-398): 4 values per body. */
+int tapas_b200_get_results(tapas_b200_ctx *ctx, double *trg4, int order, int mem);
+
+/* Partition + upward + traverse + downward + get_results in one call:
+ * the whole timestep of ex/tapas_exafmm.cxx:550-641 with mutual = 0. */
+int tapas_b200_evaluate(tapas_b200_ctx *ctx, const double *x, const double *y, const double *z,
+                        const double *q, int64_t n, int P, int ncrit, double theta, int precision,
+                        double *trg4, int order, int mem);
+
+/* FP64 direct sum on the GPU for sampled targets (the check of
+ * ex/tapas_exafmm.cxx:288-383): out4 = 4 values per target, per unit charge
+ * (field form: sum_j q_j/r and -sum_j q_j dX/r^3, no division by q_i).
+ * Bodies are the ones of the last partition; targets are original indices. */
+int tapas_b200_direct(tapas_b200_ctx *ctx, const int64_t *targets, int64_t k, double *out4,
+                      int mem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TAPAS_B200_H_ */

@@ -1,0 +1,286 @@
+"""ctypes binding of libtapas_b200.so (C ABI in include/tapas_b200.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libtapas_b200.so"
+
+OK = 0
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_CAPACITY, ERR_UNSUPPORTED, ERR_TIMEOUT = (
+    -1, -2, -3, -4, -5, -6, -7)
+HOST, DEVICE = 0, 1
+FP64, MIXED = 0, 1
+ORDER_SORTED, ORDER_ORIGINAL = 0, 1
+
+# Every symbol include/tapas_b200.h declares (checked by tests/test_abi.py).
+EXPORTS = (
+    "tapas_b200_ctx_create", "tapas_b200_ctx_destroy", "tapas_b200_set_stream",
+    "tapas_b200_set_profiling", "tapas_b200_get_timings", "tapas_b200_last_error",
+    "tapas_b200_kernel_launches", "tapas_b200_partition", "tapas_b200_tree_info",
+    "tapas_b200_get_cells", "tapas_b200_get_sorted", "tapas_b200_upward",
+    "tapas_b200_traverse", "tapas_b200_build_lists", "tapas_b200_list_info",
+    "tapas_b200_get_lists", "tapas_b200_m2l", "tapas_b200_p2p", "tapas_b200_downward",
+    "tapas_b200_get_expansions", "tapas_b200_get_results", "tapas_b200_evaluate",
+    "tapas_b200_direct",
+)
+
+
+class TreeStats(ctypes.Structure):
+    _fields_ = [("n_bodies", ctypes.c_int64), ("n_cells", ctypes.c_int64),
+                ("n_leaves", ctypes.c_int64), ("max_depth", ctypes.c_int32),
+                ("ncrit", ctypes.c_int32), ("box_lo", ctypes.c_double),
+                ("box_hi", ctypes.c_double)]
+
+
+class ListStats(ctypes.Structure):
+    _fields_ = [("n_m2l", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
+                ("n_p2p_interactions", ctypes.c_uint64),
+                ("traverse_iterations", ctypes.c_int32)]
+
+
+_TIMING_FIELDS = ("upload", "bbox_keys", "sort", "tree", "upward", "p2m", "m2m", "traverse",
+                  "list_sort", "m2l", "p2p", "downward", "l2l", "l2p", "download")
+
+
+class Timings(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_double) for f in _TIMING_FIELDS]
+
+
+class TapasError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_dbl = ctypes.c_double
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run __graft_entry__.build() "
+                          "or python tapas-reduce_b200/build.py")
+    L = ctypes.CDLL(str(LIB_PATH))
+    sig = {
+        "tapas_b200_ctx_create": [_int, ctypes.POINTER(_vp)],
+        "tapas_b200_ctx_destroy": [_vp],
+        "tapas_b200_set_stream": [_vp, _vp],
+        "tapas_b200_set_profiling": [_vp, _int],
+        "tapas_b200_get_timings": [_vp, ctypes.POINTER(Timings)],
+        "tapas_b200_partition": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int],
+        "tapas_b200_tree_info": [_vp, ctypes.POINTER(TreeStats)],
+        "tapas_b200_get_cells": [_vp] + [_vp] * 8,
+        "tapas_b200_get_sorted": [_vp, _vp, _vp],
+        "tapas_b200_upward": [_vp, _int, _int],
+        "tapas_b200_traverse": [_vp, _dbl, _int, _int],
+        "tapas_b200_build_lists": [_vp, _dbl, _int],
+        "tapas_b200_list_info": [_vp, ctypes.POINTER(ListStats)],
+        "tapas_b200_get_lists": [_vp, _vp, _vp, _vp, _vp],
+        "tapas_b200_m2l": [_vp, _int],
+        "tapas_b200_p2p": [_vp, _int],
+        "tapas_b200_downward": [_vp, _int],
+        "tapas_b200_get_expansions": [_vp, _vp, _vp],
+        "tapas_b200_get_results": [_vp, _vp, _int, _int],
+        "tapas_b200_evaluate": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int, _dbl, _int, _vp,
+                                _int, _int],
+        "tapas_b200_direct": [_vp, _vp, _i64, _vp, _int],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = _int
+    L.tapas_b200_last_error.argtypes = [_vp]
+    L.tapas_b200_last_error.restype = ctypes.c_char_p
+    L.tapas_b200_kernel_launches.argtypes = [_vp, _int]
+    L.tapas_b200_kernel_launches.restype = _i64
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    """Host numpy array or torch tensor -> (void*, mem kind)."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(_vp), HOST
+    # torch tensors (plumbing only): device pointers pass through as DEVICE.
+    if hasattr(a, "data_ptr"):
+        return _vp(a.data_ptr()), (DEVICE if a.is_cuda else HOST)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class Context:
+    """One GPU context of the library (C ABI: tapas_b200_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = _vp()
+        self._check(self._L.tapas_b200_ctx_create(device, ctypes.byref(h)), None)
+        self.h = h
+        self.n = 0
+        self.P = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.tapas_b200_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, h="self"):
+        if rc != OK:
+            hh = self.h if h == "self" else h
+            msg = self._L.tapas_b200_last_error(hh)
+            raise TapasError(rc, msg.decode() if msg else "")
+        return rc
+
+    def last_error(self) -> str:
+        return self._L.tapas_b200_last_error(self.h).decode()
+
+    # ---- configuration -------------------------------------------------
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._L.tapas_b200_set_stream(self.h, _vp(stream_handle or 0)))
+
+    def set_profiling(self, on: bool):
+        self._check(self._L.tapas_b200_set_profiling(self.h, int(on)))
+
+    def timings(self) -> dict:
+        t = Timings()
+        self._check(self._L.tapas_b200_get_timings(self.h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f in _TIMING_FIELDS}
+
+    def kernel_launches(self, reset=False) -> int:
+        return int(self._L.tapas_b200_kernel_launches(self.h, int(reset)))
+
+    # ---- tree ------------------------------------------------------------
+    def partition(self, x, y, z, q, ncrit: int = 64):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if isinstance(a, np.ndarray) else a
+                for a in (x, y, z, q)]
+        ptrs = [_ptr(a) for a in arrs]
+        mem = ptrs[0][1]
+        n = len(arrs[0]) if isinstance(arrs[0], np.ndarray) else arrs[0].numel()
+        self._keep = arrs
+        self._check(self._L.tapas_b200_partition(self.h, *[p for p, _ in ptrs], n, ncrit, mem))
+        self.n = n
+        return self.tree_info()
+
+    def tree_info(self) -> dict:
+        t = TreeStats()
+        self._check(self._L.tapas_b200_tree_info(self.h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in TreeStats._fields_}
+
+    def cells(self) -> dict:
+        C = self.tree_info()["n_cells"]
+        d = dict(key=np.zeros(C, np.uint64), leaf=np.zeros(C, np.int32), nb=np.zeros(C, np.int32),
+                 bbeg=np.zeros(C, np.int32), parent=np.zeros(C, np.int32),
+                 child0=np.zeros(C, np.int32), center=np.zeros((C, 3)), width=np.zeros((C, 3)))
+        self._check(self._L.tapas_b200_get_cells(
+            self.h, *[d[k].ctypes.data_as(_vp) for k in
+                      ("key", "leaf", "nb", "bbeg", "parent", "child0", "center", "width")]))
+        return d
+
+    def sorted_bodies(self):
+        o = np.zeros(self.n, np.int64)
+        k = np.zeros(self.n, np.uint64)
+        self._check(self._L.tapas_b200_get_sorted(self.h, o.ctypes.data_as(_vp),
+                                                  k.ctypes.data_as(_vp)))
+        return o, k
+
+    # ---- evaluation ------------------------------------------------------
+    def upward(self, P: int = 10, precision: int = FP64):
+        self.P = P
+        self._check(self._L.tapas_b200_upward(self.h, P, precision))
+
+    def build_lists(self, theta: float = 0.4, mutual: int = 0):
+        self._check(self._L.tapas_b200_build_lists(self.h, float(theta), mutual))
+        return self.list_info()
+
+    def list_info(self) -> dict:
+        t = ListStats()
+        self._check(self._L.tapas_b200_list_info(self.h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in ListStats._fields_}
+
+    def lists(self):
+        li = self.list_info()
+        mt = np.zeros(li["n_m2l"], np.int32)
+        ms = np.zeros(li["n_m2l"], np.int32)
+        pt = np.zeros(li["n_p2p"], np.int32)
+        ps = np.zeros(li["n_p2p"], np.int32)
+        self._check(self._L.tapas_b200_get_lists(self.h, *[a.ctypes.data_as(_vp)
+                                                          for a in (mt, ms, pt, ps)]))
+        return (mt, ms), (pt, ps)
+
+    def m2l(self, precision: int = FP64):
+        self._check(self._L.tapas_b200_m2l(self.h, precision))
+
+    def p2p(self, precision: int = FP64):
+        self._check(self._L.tapas_b200_p2p(self.h, precision))
+
+    def traverse(self, theta: float = 0.4, mutual: int = 0, precision: int = FP64):
+        self._check(self._L.tapas_b200_traverse(self.h, float(theta), mutual, precision))
+
+    def downward(self, precision: int = FP64):
+        self._check(self._L.tapas_b200_downward(self.h, precision))
+
+    def expansions(self):
+        C = self.tree_info()["n_cells"]
+        nt = self.P * (self.P + 1) // 2
+        M = np.zeros((C, nt, 2))
+        L = np.zeros((C, nt, 2))
+        self._check(self._L.tapas_b200_get_expansions(self.h, M.ctypes.data_as(_vp),
+                                                      L.ctypes.data_as(_vp)))
+        return M[..., 0] + 1j * M[..., 1], L[..., 0] + 1j * L[..., 1]
+
+    def results(self, order: int = ORDER_ORIGINAL, out=None):
+        if out is None:
+            out = np.zeros((self.n, 4))
+        p, mem = _ptr(out)
+        self._check(self._L.tapas_b200_get_results(self.h, p, order, mem))
+        return out
+
+    def evaluate(self, x, y, z, q, P=10, ncrit=64, theta=0.4, precision=FP64,
+                 order=ORDER_ORIGINAL, out=None):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if isinstance(a, np.ndarray) else a
+                for a in (x, y, z, q)]
+        ptrs = [_ptr(a) for a in arrs]
+        mem = ptrs[0][1]
+        n = len(arrs[0]) if isinstance(arrs[0], np.ndarray) else arrs[0].numel()
+        if out is None:
+            out = np.zeros((n, 4))
+        op, omem = _ptr(out)
+        if omem != mem:
+            raise ValueError("inputs and output must live in the same memory kind")
+        self._keep = arrs
+        self.P = P
+        self._check(self._L.tapas_b200_evaluate(self.h, *[p for p, _ in ptrs], n, P, ncrit,
+                                                float(theta), precision, op, order, mem))
+        self.n = n
+        return out
+
+    def direct(self, targets) -> np.ndarray:
+        tg = np.ascontiguousarray(targets, dtype=np.int64)
+        out = np.zeros((len(tg), 4))
+        self._check(self._L.tapas_b200_direct(self.h, tg.ctypes.data_as(_vp), len(tg),
+                                              out.ctypes.data_as(_vp), HOST))
+        return out

@@ -1,0 +1,24 @@
+// Mixed-precision evaluation path (TAPAS_B200_MIXED).
+//
+// Near field: FP32 compensated P2P (p2p.cu, p2p_mixed).  Far field: the
+// expansion passes keep their FP64 form; the near-field result is per unit
+// charge, so L2P adds to it without the reference's division by q_i.
+#include "kernels.cuh"
+#include "mixed.cuh"
+
+namespace tb {
+
+int upward_mixed(tapas_b200_ctx *ctx, int P) { return upward_fp64(ctx, P); }
+
+int m2l_mixed(tapas_b200_ctx *ctx) { return m2l_fp64(ctx); }
+
+int downward_mixed(tapas_b200_ctx *ctx) { return downward_fp64(ctx); }
+
+int mixed_sync_fp64_view(tapas_b200_ctx *ctx) {
+  (void)ctx;
+  return TAPAS_B200_OK;
+}
+
+void mixed_release(tapas_b200_ctx *ctx) { ctx->rel4.release(); }
+
+}  // namespace tb

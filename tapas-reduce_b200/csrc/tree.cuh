@@ -1,0 +1,9 @@
+// Octree construction (bbox, keys, sort, cells) on ctx->stream.
+#pragma once
+#include "common.cuh"
+
+namespace tb {
+int ensure_cells(tapas_b200_ctx *ctx, int64_t need, int64_t used);
+// Builds the tree of the bodies already in ctx->x/y/z/q (ctx->n of them).
+int build_tree(tapas_b200_ctx *ctx, int ncrit);
+}  // namespace tb

@@ -1,0 +1,76 @@
+"""Generates the golden fixtures in this directory from the UNMODIFIED reference.
+
+Each case runs the reference ExaFMM/Tapas example (built from its own sources
+by ``make -C oracle ref`` into oracle/_ref/, see oracle/ref_driver.cxx) on a
+seeded synthetic body set and stores its inputs and outputs:
+
+* ``x, y, z, q``            inputs (original order)
+* ``trg``                   reference TRG per body, ORIGINAL order (pot, ax, ay, az)
+* ``order``                 original index of each body in the reference's sorted order
+* ``cell_key/leaf/nb/bid``  cells sorted by key; ``cell_center``, ``cell_width``
+* ``M``, ``L``              per-cell expansions (small cases only)
+* ``n_m2l``, ``n_p2p_interactions``  the reference's -DCOUNT counters
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import importlib.util
+import pathlib
+import sys
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle"))
+import oracle  # noqa: E402
+
+spec = importlib.util.spec_from_file_location("ds", ROOT / "tapas-reduce_b200" / "datasets.py")
+ds = importlib.util.module_from_spec(spec)
+spec.loader.exec_module(ds)
+
+# name: (distribution, n, seed, P, ncrit, theta, keep_expansions)
+CASES = {
+    "cube_n2000_p10": ("uniform_cube", 2000, 11, 10, 32, 0.4, False),
+    "plummer_n3000_p8": ("plummer", 3000, 12, 8, 24, 0.5, False),
+    "sphere_n2500_p6": ("sphere_surface", 2500, 13, 6, 16, 0.35, False),
+    "gauss_n1500_p4": ("two_gaussians", 1500, 14, 4, 8, 0.6, False),
+    "cube_n400_p6_ML": ("uniform_cube", 400, 15, 6, 16, 0.4, True),
+    "cube_n300_ncrit1_p4": ("uniform_cube", 300, 16, 4, 1, 0.5, False),
+    "tiny_n1": ("uniform_cube", 1, 17, 4, 64, 0.4, True),
+    "tiny_n2": ("uniform_cube", 2, 18, 4, 1, 0.4, True),
+    "tiny_n7": ("plummer", 7, 19, 6, 2, 0.4, True),
+    "root_leaf_n50": ("uniform_cube", 50, 20, 8, 64, 0.4, True),
+}
+
+
+def make(name, dist, n, seed, P, ncrit, theta, keep):
+    x, y, z, q = ds.make(dist, n, seed)
+    R = oracle.run_reference(x, y, z, q, P=P, ncrit=ncrit, theta=theta)
+    b = R["bodies"]
+    trg = np.empty((n, 4))
+    trg[b["ibody"]] = b["trg"]
+    c = R["cells"]
+    out = dict(x=x, y=y, z=z, q=q, P=P, ncrit=ncrit, theta=theta, trg=trg,
+               order=b["ibody"].astype(np.int64),
+               cell_key=c["key"], cell_leaf=c["leaf"], cell_nb=c["nb"], cell_bid=c["bid"],
+               cell_center=c["center"], cell_width=c["width"],
+               n_m2l=R["n_m2l"], n_p2p_interactions=R["n_p2p_interactions"])
+    if keep:
+        out["M"] = c["M"][..., 0] + 1j * c["M"][..., 1]
+        out["L"] = c["L"][..., 0] + 1j * c["L"][..., 1]
+    np.savez_compressed(pathlib.Path(__file__).parent / f"{name}.npz", **out)
+    print(name, n, "cells", len(c), "m2l", R["n_m2l"], "p2p", R["n_p2p_interactions"])
+
+
+if __name__ == "__main__":
+    import subprocess
+    oracle.build_reference(quiet=False)
+    for name, args in CASES.items():
+        try:
+            make(name, *args)
+        except subprocess.CalledProcessError as e:
+            # The reference aborts when the root cell is itself a leaf
+            # (n <= ncrit): its Map direction probe calls subcell() on it
+            # ("Cell::subcell(int) is called for a leaf cell").  No golden.
+            print(name, "reference failed:", e.returncode)
