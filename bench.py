@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the Tapas N-body evaluation path on B200.
+
+Workload (one step = one full FMM evaluation: octree build, upward pass,
+dual-tree traversal with M2L + P2P, downward pass):
+  N = 16,000,000 bodies uniform on the unit sphere surface, charges U[-1,1]
+  minus their mean, requested relative-L2 potential error 1e-6.  Parameters
+  (P, theta, ncrit) come from the parameter chooser; the result is verified
+  against an FP64 direct sum on 4,000 sampled targets.
+
+Printed JSON line (rank 0):
+  value       particles/s of the mixed form, inputs resident in HBM
+  e2e         the same through the C-ABI evaluate() call with pinned HOST
+              buffers: host->device copy of the bodies and device->host copy of
+              the results inside the timed region
+  fp64        the plain FP64 form (same chooser tolerance rule) for reference
+  roofline    the dominant kernel of the step against its bound
+  cpu_baseline  the reference's own CPU implementation (oracle/_ref, built from
+              the reference sources) on a bounded sample of the same workload
+
+Multi-GPU: replicas only (the path is one tree per GPU); each rank evaluates its
+own seeded body set, value = all ranks' bodies / max-over-ranks time.
+``--impl reference`` times the reference CPU implementation instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+METRIC = "FMM particles/s at 1e-6 rel-L2: mixed+learned vs plain FP64 on 1 B200"
+WORKLOAD = "sphere_surface"
+
+
+def load_package():
+    if "tapas_reduce_b200" in sys.modules:
+        return sys.modules["tapas_reduce_b200"]
+    pkg_dir = ROOT / "tapas-reduce_b200"
+    spec = importlib.util.spec_from_file_location(
+        "tapas_reduce_b200", pkg_dir / "__init__.py", submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["tapas_reduce_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    return oracle
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nme in enumerate(names):
+                if r[5 + i].lower().startswith("active"):
+                    reasons.add(nme)
+        out["sm_mhz"] = float(np.median(sm)) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        os.unlink(self.path)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = tdist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# reference CPU implementation (oracle/_ref, built from the reference sources)
+# ---------------------------------------------------------------------------
+REF_SAMPLE_N = 50_000
+REF_P, REF_THETA, REF_NCRIT = 12, 0.3, 64
+
+
+def cpu_reference_run(tb, orc, n=REF_SAMPLE_N, seed=77):
+    """One evaluation of the reference FMM on a bounded sample of the
+    workload (same distribution, n bodies) on one host core; particles/s."""
+    x, y, z, q = tb.datasets.make(WORKLOAD, n, seed)
+    if orc.reference_available(REF_P):
+        r = orc.run_reference(x, y, z, q, P=REF_P, ncrit=REF_NCRIT, theta=REF_THETA)
+        t = r["times"]
+        secs = t["tree"] + t["upward"] + t["traverse"] + t["downward"]
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        orc.Oracle(x, y, z, q, P=REF_P, ncrit=REF_NCRIT, theta=REF_THETA)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    return n / secs, kind, secs
+
+
+def cpu_baseline_obj(value, kind, secs):
+    return {"value": value, "unit": "particles/s", "cores": 1, "kind": kind,
+            "sample": f"{REF_SAMPLE_N} bodies of the same sphere-surface workload, "
+                      f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (meets 1e-6 on it), "
+                      f"1 rank x 1 thread (the reference's Serial threading), {secs:.2f} s"}
+
+
+def run_reference_arm(args):
+    world, rank, _, pg = dist_setup(args)
+    if rank != 0:
+        return 0
+    tb = load_package()
+    orc = load_oracle()
+    vals = []
+    kind = secs = None
+    for i in range(args.warmup + args.steps):
+        v, kind, secs = cpu_reference_run(tb, orc, seed=77 + i)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": REF_SAMPLE_N / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD} sample n={REF_SAMPLE_N}", "P": REF_P,
+                       "theta": REF_THETA, "ncrit": REF_NCRIT},
+            "cpu_baseline": cpu_baseline_obj(value, kind, secs),
+            "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def choose(tb, n, tol, precision):
+    from importlib import import_module
+    chooser = import_module("tapas_reduce_b200.chooser")
+    return chooser.choose_params(n=n, tol=tol, precision=precision)
+
+
+def time_steps(ctx, fn, steps, warmup, stream_sync):
+    for _ in range(warmup):
+        fn()
+    stream_sync()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        fn()
+    stream_sync()
+    return (time.perf_counter() - t0) / steps
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=16_000_000)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--targets", type=int, default=4000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    tb = load_package()
+    n = args.n
+    x, y, z, q = tb.datasets.make(WORKLOAD, n, seed=5 + 1000 * rank)
+    tg = tb.datasets.sample_targets(n, args.targets, seed=99 + rank)
+    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
+    pinned = [torch.from_numpy(a).pin_memory() for a in (x, y, z, q)]
+    out_dev = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    out_pin = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    ctx = tb.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    orc = load_oracle()
+
+    prm = choose(tb, n, args.tol, "mixed")
+    P, theta, ncrit = prm["P"], prm["theta"], prm["ncrit"]
+    torch.cuda.synchronize()
+
+    def step_dev():
+        ctx.evaluate(*dev, P=P, ncrit=ncrit, theta=theta, precision=tb.MIXED, out=out_dev)
+
+    def step_e2e():
+        ctx.evaluate(*pinned, P=P, ncrit=ncrit, theta=theta, precision=tb.MIXED, out=out_pin)
+
+    sync = stream.synchronize
+    # ---- timed region: device-resident inputs, CUDA events on our stream ----
+    for _ in range(args.warmup):
+        step_dev()
+    ctx.set_profiling(True)
+    ctx.kernel_launches(reset=True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phase_acc = {}
+    barrier(pg)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step_dev()
+            for k, v in ctx.timings().items():
+                phase_acc[k] = phase_acc.get(k, 0.0) + v
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = ctx.kernel_launches() // args.steps
+    ctx.set_profiling(False)
+    clocks = clk.summary()
+    ms_max = max_over_ranks(pg, ms)
+    n_total = sum_over_ranks(pg, n)
+    value = n_total / (ms_max * 1e-3)
+    phases = {k: v / args.steps for k, v in phase_acc.items()}
+    li = ctx.list_info()
+    ti = ctx.tree_info()
+
+    # ---- verification against FP64 direct sum on sampled targets ----
+    res = out_dev.cpu().numpy()
+    d = ctx.direct(tg)
+    err = orc.rel_l2(res[tg], d)
+
+    # ---- e2e through the C-ABI call with pinned host buffers ----
+    for _ in range(2):
+        step_e2e()
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_steps = max(1, min(args.steps, 3))
+    for _ in range(e_steps):
+        step_e2e()
+    e2e_s = (time.perf_counter() - t0) / e_steps
+    e2e_s = max_over_ranks(pg, e2e_s)
+    e2e = {"value": n_total / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 4 * 8 * n,
+           "d2h_bytes_per_step": 4 * 8 * n}
+
+    # ---- plain FP64 form at the same tolerance rule ----
+    fp64 = None
+    if not args.no_fp64:
+        p64 = choose(tb, n, args.tol, "fp64")
+
+        def step64():
+            ctx.evaluate(*dev, P=p64["P"], ncrit=p64["ncrit"], theta=p64["theta"],
+                         precision=tb.FP64, out=out_dev)
+        step64()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(2):
+            step64()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = max_over_ranks(pg, e0.elapsed_time(e1) / 2)
+        err64 = orc.rel_l2(out_dev.cpu().numpy()[tg], d)
+        fp64 = {"value": n_total / (ms64 * 1e-3), "unit": "particles/s", "ms_per_step": ms64,
+                "params": p64, "rel_l2_pot": err64[0], "rel_l2_acc": err64[1],
+                "mixed_speedup": ms64 / ms_max}
+
+    # ---- roofline of the dominant kernel ----
+    roofline = roofline_obj(phases, li, ti, P, tb)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, kind, secs = cpu_reference_run(tb, orc)
+        cpu = cpu_baseline_obj(v, kind, secs)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64", "data": "synthetic",
+                "config": {"workload": f"{WORKLOAD} N={n} q=U[-1,1]-mean tol={args.tol}",
+                           "bodies_per_gpu": n, "P": P, "theta": theta, "ncrit": ncrit,
+                           "chooser": prm.get("source"), "precision": "mixed",
+                           "l2_flush": "inputs larger than L2 (512 MB of bodies per step)",
+                           "parallelism": f"replicas x{world}"},
+                "accuracy": {"rel_l2_pot": err[0], "rel_l2_acc": err[1],
+                             "targets": int(len(tg)), "meets_tol": bool(err[0] <= args.tol)},
+                "e2e": e2e, "fp64": fp64, "phases_ms": phases,
+                "work": {"n_m2l": li["n_m2l"], "n_p2p_interactions": li["n_p2p_interactions"],
+                         "n_cells": ti["n_cells"], "max_depth": ti["max_depth"]},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def roofline_obj(phases, li, ti, P, tb):
+    """Dominant kernel of the step and its roofline."""
+    peaks, src = _peaks()
+    from importlib import import_module
+    rl = import_module("tapas_reduce_b200.roofline")
+    return rl.dominant(phases, li, ti, P, peaks, src)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

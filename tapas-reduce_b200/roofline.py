@@ -1,0 +1,64 @@
+"""Roofline bookkeeping for the evaluation phases.
+
+Algorithmic work per unit (the figures `achieved` is computed from):
+* P2P   : 20 flop per body-pair interaction (the reference's convention,
+          sample/barnes-hut/bh.cc:407, exafmm gpu/serial.cu:65); bound by the
+          FP32 pipe (mixed) or FP64 pipe (plain).
+* M2L   : 8 * sum_{j<P} (j+1)(P-j)^2 flop per translation (the reference's
+          complex multiply-add count in LaplaceSphericalCPU_tapas.h:227-270);
+          FP64 pipe (plain) or tensor pipe (mixed, split TF32).
+* sort  : 8 LSD passes x (read + write of u64 key + u32 index) = 192 B/body;
+          keys: 32 B read + 12 B written per body; HBM bound.
+Peaks: HBM from MEASURED_PEAKS.json; FP32/FP64 CUDA-core peaks are nominal
+(148 SMs x 128 FP32 / 64 FP64 FMA per clock x 2 x max SM clock), no measured
+figure exists for them.
+"""
+from __future__ import annotations
+
+
+def m2l_flops_per_translation(P: int) -> int:
+    return 8 * sum((j + 1) * (P - j) ** 2 for j in range(P))
+
+
+def nominal_tflops(kind: str, sm_mhz: float, sms: int = 148) -> float:
+    lanes = {"fp32": 128, "fp64": 64}[kind]
+    return sms * lanes * 2 * sm_mhz * 1e6 / 1e12
+
+
+def dominant(phases: dict, lists: dict, tree: dict, P: int, peaks: dict, peak_src: str,
+             precision: str = "mixed") -> dict:
+    cand = {k: phases.get(k, 0.0) for k in ("bbox_keys", "sort", "tree", "p2m", "m2m",
+                                            "traverse", "list_sort", "m2l", "p2p", "l2l",
+                                            "l2p")}
+    name = max(cand, key=cand.get)
+    ms = cand[name]
+    smx = float(peaks.get("sm_max_mhz", 1965.0))
+    out = {"kernel": name, "ms": ms}
+    if ms <= 0:
+        return out
+    n = tree.get("n_bodies", 0)
+    if name == "p2p":
+        fl = 20.0 * lists["n_p2p_interactions"]
+        kind = "fp32" if precision == "mixed" else "fp64"
+        peak = nominal_tflops(kind, smx)
+        ach = fl / (ms * 1e-3) / 1e12
+        out.update(bound=kind, achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
+                   peak_source=f"nominal {kind} at {smx:.0f} MHz", traffic=None,
+                   work=f"{lists['n_p2p_interactions']} interactions x 20 flop")
+    elif name == "m2l":
+        fl = float(m2l_flops_per_translation(P)) * lists["n_m2l"]
+        ach = fl / (ms * 1e-3) / 1e12
+        peak = nominal_tflops("fp64", smx)
+        out.update(bound="fp64", achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
+                   peak_source=f"nominal fp64 at {smx:.0f} MHz", traffic=None,
+                   work=f"{lists['n_m2l']} translations x {m2l_flops_per_translation(P)} flop")
+    else:
+        per = {"sort": 192.0, "bbox_keys": 44.0 + 48.0, "tree": 16.0}.get(name)
+        if per is None:
+            out.update(bound="latency", note="no algorithmic byte/flop model for this phase")
+            return out
+        gbs = per * n / (ms * 1e-3) / 1e9
+        peak = float(peaks["hbm_gbs"])
+        out.update(bound="hbm", achieved=gbs, peak=peak, unit="GB/s", frac=gbs / peak,
+                   peak_source=peak_src, traffic=None, work=f"{per} B/body x {n}")
+    return out
