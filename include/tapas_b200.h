@@ -73,6 +73,10 @@ typedef struct {
   int64_t n_p2p;               /* P2P leaf pairs with both leaves non-empty        */
   uint64_t n_p2p_interactions; /* sum over leaf pairs of nb_i * nb_j              */
   int32_t traverse_iterations;
+  /* Mixed-form M2L of the last tapas_b200_m2l(MIXED) call: */
+  int64_t n_m2l_tc;            /* translations evaluated on the tensor cores       */
+  int64_t tc_classes;          /* offset classes run as GEMMs                      */
+  int64_t tc_tiles;            /* 128-translation GEMM tiles                       */
 } tapas_b200_list_stats;
 
 /* Phase timings of the last calls, milliseconds, measured with CUDA events on
@@ -80,6 +84,9 @@ typedef struct {
 typedef struct {
   double upload, bbox_keys, sort, tree, upward, p2m, m2m, traverse, list_sort, m2l, p2p,
       downward, l2l, l2p, download;
+  double m2l_fp64;  /* M2L pairs evaluated by the FP64 kernel                 */
+  double m2l_tc;    /* M2L tensor-core GEMM kernel (mixed form)              */
+  double m2l_setup; /* mixed-form M2L: class sort, operators, normalisation  */
 } tapas_b200_timings;
 
 /* ---- context ------------------------------------------------------------- */
@@ -92,6 +99,11 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx);
 /* Use `stream` (a cudaStream_t) for all later work; NULL restores the context's own. */
 int tapas_b200_set_stream(tapas_b200_ctx *ctx, void *stream);
 int tapas_b200_set_profiling(tapas_b200_ctx *ctx, int on);
+/* on = 1: the traversal keeps the pairs that involve empty cells, exactly as
+ * the reference's FMM_DTT visits them (ex/tapas_exafmm.cxx:209-286), so the
+ * lists equal the reference's; on = 0 (default): such pairs, which contribute
+ * nothing, are dropped.  Results are the same either way. */
+int tapas_b200_set_reference_lists(tapas_b200_ctx *ctx, int on);
 int tapas_b200_get_timings(tapas_b200_ctx *ctx, tapas_b200_timings *out);
 /* Message of the last failing call on this context ("" if none). Thread-local
  * fallback when ctx is NULL (e.g. ctx_create failure). */

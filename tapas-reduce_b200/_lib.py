@@ -22,7 +22,8 @@ ORDER_SORTED, ORDER_ORIGINAL = 0, 1
 # Every symbol include/tapas_b200.h declares (checked by tests/test_abi.py).
 EXPORTS = (
     "tapas_b200_ctx_create", "tapas_b200_ctx_destroy", "tapas_b200_set_stream",
-    "tapas_b200_set_profiling", "tapas_b200_get_timings", "tapas_b200_last_error",
+    "tapas_b200_set_profiling", "tapas_b200_set_reference_lists", "tapas_b200_get_timings",
+    "tapas_b200_last_error",
     "tapas_b200_kernel_launches", "tapas_b200_partition", "tapas_b200_tree_info",
     "tapas_b200_get_cells", "tapas_b200_get_sorted", "tapas_b200_upward",
     "tapas_b200_traverse", "tapas_b200_build_lists", "tapas_b200_list_info",
@@ -42,11 +43,13 @@ class TreeStats(ctypes.Structure):
 class ListStats(ctypes.Structure):
     _fields_ = [("n_m2l", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
                 ("n_p2p_interactions", ctypes.c_uint64),
-                ("traverse_iterations", ctypes.c_int32)]
+                ("traverse_iterations", ctypes.c_int32), ("n_m2l_tc", ctypes.c_int64),
+                ("tc_classes", ctypes.c_int64), ("tc_tiles", ctypes.c_int64)]
 
 
 _TIMING_FIELDS = ("upload", "bbox_keys", "sort", "tree", "upward", "p2m", "m2m", "traverse",
-                  "list_sort", "m2l", "p2p", "downward", "l2l", "l2p", "download")
+                  "list_sort", "m2l", "p2p", "downward", "l2l", "l2p", "download", "m2l_fp64",
+                  "m2l_tc", "m2l_setup")
 
 
 class Timings(ctypes.Structure):
@@ -79,6 +82,7 @@ def lib():
         "tapas_b200_ctx_destroy": [_vp],
         "tapas_b200_set_stream": [_vp, _vp],
         "tapas_b200_set_profiling": [_vp, _int],
+        "tapas_b200_set_reference_lists": [_vp, _int],
         "tapas_b200_get_timings": [_vp, ctypes.POINTER(Timings)],
         "tapas_b200_partition": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int],
         "tapas_b200_tree_info": [_vp, ctypes.POINTER(TreeStats)],
@@ -164,6 +168,10 @@ class Context:
 
     def set_profiling(self, on: bool):
         self._check(self._L.tapas_b200_set_profiling(self.h, int(on)))
+
+    def set_reference_lists(self, on: bool):
+        """Keep the traversal's pairs with empty cells, as the reference does."""
+        self._check(self._L.tapas_b200_set_reference_lists(self.h, int(on)))
 
     def timings(self) -> dict:
         t = Timings()

@@ -204,6 +204,12 @@ int tapas_b200_set_profiling(tapas_b200_ctx *ctx, int on) {
   return TAPAS_B200_OK;
 }
 
+int tapas_b200_set_reference_lists(tapas_b200_ctx *ctx, int on) {
+  TB_TRY(check_ctx(ctx));
+  ctx->reference_lists = on != 0;  // applies to the next list construction
+  return TAPAS_B200_OK;
+}
+
 int tapas_b200_get_timings(tapas_b200_ctx *ctx, tapas_b200_timings *out) {
   TB_TRY(check_ctx(ctx));
   if (!out) return TAPAS_B200_ERR_ARG;
@@ -363,6 +369,9 @@ int tapas_b200_list_info(tapas_b200_ctx *ctx, tapas_b200_list_stats *out) {
   out->n_p2p = ctx->n_p2p;
   out->n_p2p_interactions = ctx->n_p2p_int;
   out->traverse_iterations = ctx->trav_iters;
+  out->n_m2l_tc = ctx->n_m2l_tc;
+  out->tc_classes = ctx->tc_classes;
+  out->tc_tiles = ctx->tc_tiles;
   return TAPAS_B200_OK;
 }
 
@@ -400,6 +409,7 @@ int tapas_b200_m2l(tapas_b200_ctx *ctx, int precision) {
     set_error(ctx, "m2l: needs upward and build_lists first");
     return TAPAS_B200_ERR_STATE;
   }
+  PhaseTimer t(ctx, &ctx->timings.m2l);
   if (precision == TAPAS_B200_MIXED) TB_TRY(m2l_mixed(ctx));
   else TB_TRY(m2l_fp64(ctx));
   ctx->have_L = true;

@@ -98,6 +98,23 @@ struct HBuf {
   }
 };
 
+// Work state of the tensor-core M2L (m2l_tc.cu).
+struct TcState {
+  DBuf<uint64_t> keys, keys_alt, tc_keys;
+  DBuf<uint32_t> vals, vals_alt;
+  DBuf<uint8_t> use64;
+  DBuf<int32_t> flag, scan, seg_start, tcflag, tcid, ntiles, tile_off;
+  DBuf<int4> items;
+  DBuf<float> ops_hi, ops_lo, Mt, Lt;
+  DBuf<int> err;
+  void release() {
+    keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();
+    use64.release(); flag.release(); scan.release(); seg_start.release(); tcflag.release();
+    tcid.release(); ntiles.release(); tile_off.release(); items.release(); ops_hi.release();
+    ops_lo.release(); Mt.release(); Lt.release(); err.release();
+  }
+};
+
 }  // namespace tb
 
 // ---------------------------------------------------------------------------
@@ -151,6 +168,7 @@ struct tapas_b200_ctx {
   uint64_t n_p2p_int = 0;
   int trav_iters = 0;
   int list_shift = 1;                   // packed list key = target << shift | source
+  bool reference_lists = false;         // keep pairs with empty cells, as the reference visits them
   tb::DBuf<int32_t> m2l_off, p2p_off;   // CSR by target cell, ncells+1
   tb::DBuf<int32_t> m2l_tlist, p2p_tlist; // targets having list entries
   int64_t n_m2l_targets = 0, n_p2p_targets = 0;
@@ -159,7 +177,14 @@ struct tapas_b200_ctx {
   int P = 0;
   int precision = TAPAS_B200_FP64;       // of the expansion passes (set by upward)
   int near_precision = TAPAS_B200_FP64;  // of the last P2P: FP64 sums carry q_i, mixed do not
-  tb::DBuf<float4> rel4;                // mixed: (x - c_leaf, y - c_leaf, z - c_leaf, q) FP32
+  tb::DBuf<float4> rel4;                // mixed: hi part of (x,y,z) - c_leaf, and q, FP32
+  tb::DBuf<float4> rel_lo;              // mixed: lo part of (x,y,z) - c_leaf, FP32
+  tb::DBuf<uint64_t> p2p_wkey, p2p_wkey_alt;  // P2P work order: keys
+  tb::DBuf<uint32_t> p2p_order, p2p_order_alt;  // target leaves by decreasing work
+  tb::DBuf<int> p2p_counter;            // P2P work-queue head
+  tb::TcState tc;                       // mixed: tensor-core M2L work state
+  const uint8_t *m2l_use = nullptr;     // FP64 M2L: evaluate only pairs with use[e] != 0
+  int64_t tc_classes = 0, tc_tiles = 0, tc_segments = 0, n_m2l_tc = 0;
   bool have_M = false, have_L = false;
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
 

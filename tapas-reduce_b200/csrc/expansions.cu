@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
 // ---------------------------------------------------------------------------
 template <int P>
 __global__ void __launch_bounds__(kThreads) m2m_kernel(
-    int64_t a, int64_t cnt, const int32_t *__restrict__ cleaf, const int32_t *__restrict__ cchild,
-    const double *__restrict__ ccen, double2 *__restrict__ M) {
+    int64_t a, int64_t cnt, const int32_t *__restrict__ cleaf, const int32_t *__restrict__ cnb,
+    const int32_t *__restrict__ cchild, const double *__restrict__ ccen, double2 *__restrict__ M) {
   using S = Sizes<P>;
   __shared__ cd Ysm[kWarps][S::NY];
   __shared__ cd Msm[kWarps][S::NT];
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kThreads) m2m_kernel(
   const int64_t w = (int64_t)blockIdx.x * kWarps + wi;
   if (w >= cnt) return;
   const int64_t c = a + w;
-  if (cleaf[c]) return;
+  if (cleaf[c] || cnb[c] == 0) return;  // an empty cell's M stays zero
   cd *Y = Ysm[wi];
   cd *Mj = Msm[wi];
   cd acc[S::R];
@@ -184,7 +184,7 @@ template <int P>
 __global__ void __launch_bounds__(kThreads) m2l_kernel(
     int64_t ncells, const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
     uint64_t src_mask, const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
-    const double2 *__restrict__ M, double2 *__restrict__ L) {
+    const double2 *__restrict__ M, double2 *__restrict__ L, const uint8_t *__restrict__ use) {
   using S = Sizes<P>;
   __shared__ cd Ysm[kWarps][S::NY];
   __shared__ cd Msm[kWarps][S::NT];
@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
   for (int e = e0; e < e1; e++) {
     const int s = (int)(list[e] & src_mask);
     if (cnb[s] == 0) continue;  // M of an empty cell is exactly zero
+    if (use && !use[e]) continue;  // pair evaluated elsewhere (tensor-core classes)
     double rho, alpha, beta;
     cart2sph(tx - ccen[3 * s], ty - ccen[3 * s + 1], tz - ccen[3 * s + 2], rho, alpha, beta);
     const double x = cos(alpha), y = sin(alpha);
@@ -408,7 +409,7 @@ int upward_P(tapas_b200_ctx *ctx) {
     const int64_t a = ctx->level_off[lev], cnt = ctx->level_off[lev + 1] - a;
     if (cnt <= 0) continue;
     m2m_kernel<P><<<(unsigned)((cnt + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        a, cnt, ctx->cleaf.p, ctx->cchild.p, ctx->ccen.p, ctx->M.p);
+        a, cnt, ctx->cleaf.p, ctx->cnb.p, ctx->cchild.p, ctx->ccen.p, ctx->M.p);
     TB_LAUNCH_CHECK(ctx);
   }
   return TAPAS_B200_OK;
@@ -421,10 +422,11 @@ int m2l_P(tapas_b200_ctx *ctx) {
   const int64_t C = ctx->ncells;
   TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
   TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
-  PhaseTimer t(ctx, &ctx->timings.m2l);
+  PhaseTimer t(ctx, &ctx->timings.m2l_fp64);
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   m2l_kernel<P><<<(unsigned)((C + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-      C, ctx->m2l_off.p, ctx->m2l.p, mask, ctx->cnb.p, ctx->ccen.p, ctx->M.p, ctx->L.p);
+      C, ctx->m2l_off.p, ctx->m2l.p, mask, ctx->cnb.p, ctx->ccen.p, ctx->M.p, ctx->L.p,
+      ctx->m2l_use);
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
 }
@@ -468,7 +470,19 @@ int downward_P(tapas_b200_ctx *ctx) {
   return TAPAS_B200_ERR_UNSUPPORTED;
 
 int upward_fp64(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_P) }
-int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
+int m2l_fp64(tapas_b200_ctx *ctx) {
+  ctx->m2l_use = nullptr;
+  TB_DISPATCH_P(ctx->P, m2l_P)
+}
+
+static int m2l_fp64_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
+
+int m2l_fp64_masked(tapas_b200_ctx *ctx, const uint8_t *use) {
+  ctx->m2l_use = use;
+  const int rc = m2l_fp64_dispatch(ctx);
+  ctx->m2l_use = nullptr;
+  return rc;
+}
 int downward_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, downward_P) }
 
 }  // namespace tb

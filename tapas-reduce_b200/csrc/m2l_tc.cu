@@ -1,0 +1,708 @@
+// M2L on the 5th-generation tensor cores (mixed form).
+//
+// The spherical M2L (ex/LaplaceSphericalCPU_tapas.h:208-273) is real-linear
+// in the source multipole: with M and L stored as real vectors of length
+// K = 2*P(P+1)/2 (re, im per coefficient), L_t += T(c_t - c_s) M_s.  After
+// scaling every cell's M_n by w^-n and L_j by w^(j+1) (w = cell width), T
+// depends only on the translation's class: the level difference
+// delta = depth_t - depth_s and the integer offset
+// D = (c_t - c_s) / (w_min / 2) (centres of cells are odd multiples of half
+// their width from the cube corner, so D is an integer vector).  Every M2L
+// pair of a class is then one column of a dense GEMM
+//     Lt[:, pairs] += T_class (K x K) * Mt[:, sources of pairs].
+//
+// Execution:
+//  1. classify: class key per M2L pair; stable radix sort of the pairs by key
+//     (the target order inside a class is kept); segments = classes.
+//  2. classes with >= kTcMin pairs run on the tensor cores; the rest (and
+//     pairs whose offset does not fit the key) stay on the FP64 kernel.
+//  3. per tensor-core class the real K x K operator is built in FP64 from the
+//     unit-width singular harmonics and split into TF32 hi + lo parts, laid
+//     out as K-major core matrices (8 rows x 16 bytes) ready for smem.
+//  4. GEMM kernel: a CTA takes tiles of 128 pairs of one class; K is streamed
+//     in chunks through a 2-stage shared-memory ring; one thread issues
+//     tcgen05.mma kind::tf32 (M=128 rows of T per M-tile, N=128 pairs, K=8)
+//     three times per k-step (hi*hi + lo*hi + hi*lo: split-precision
+//     "3xTF32", FP32 accumulation in TMEM); completion via tcgen05.commit to
+//     an mbarrier (bounded waits); the epilogue reads TMEM with tcgen05.ld and
+//     adds each column into its target's Lt with fire-and-forget reductions.
+//  5. Lt is rescaled and added into the FP64 L.
+#include <algorithm>
+#include <optional>
+
+#include "expansions.cuh"
+#include "kernels.cuh"
+#include "m2l_tc.cuh"
+#include "primitives.cuh"
+
+namespace tb {
+namespace {
+
+constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor cores
+constexpr int kNTile = 128;        // pairs per tile (MMA N)
+constexpr int kThreadsTc = 256;    // 8 warps
+constexpr uint64_t kKeyEmpty = 0xFFFFFFFFFFFFull;  // source has no bodies: no work
+constexpr uint64_t kKeyRare = 0xFFFFFFFFFFFEull;   // offset outside the key range: FP64
+constexpr int kOffBias = 8192;
+
+template <int P>
+struct TcShape {
+  static constexpr int NT = P * (P + 1) / 2;
+  static constexpr int K = 2 * NT;                    // real dimension
+  static constexpr int MT = (K + 127) / 128;          // M-tiles of 128 operator rows
+  static constexpr int MP = MT * 128;
+  static constexpr int KC = MT <= 2 ? 32 : 16;        // K chunk per stage
+  static constexpr int KP = ((K + KC - 1) / KC) * KC; // padded K
+  static constexpr int NKC = KP / KC;
+  static constexpr int TMEM_COLS = MT == 1 ? 128 : (MT == 2 ? 256 : 512);
+  // one stage: A hi/lo (MP x KC) + B hi/lo (128 x KC) floats
+  static constexpr int STAGE_FLOATS = 2 * MP * KC + 2 * kNTile * KC;
+  static constexpr size_t SMEM = 2 * STAGE_FLOATS * sizeof(float) + 4096;
+};
+
+// ---------------------------------------------------------------------------
+// classification
+// ---------------------------------------------------------------------------
+__global__ void classify_pairs(int64_t n, const uint64_t *__restrict__ list, int shift,
+                               const int32_t *__restrict__ cnb,
+                               const int32_t *__restrict__ clevel,
+                               const double *__restrict__ cmin, const double *__restrict__ cmax,
+                               const double *__restrict__ ccen, uint64_t *__restrict__ keys,
+                               uint32_t *__restrict__ vals) {
+  const uint64_t mask = (1ull << shift) - 1;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = list[e];
+    const int t = (int)(v >> shift), s = (int)(v & mask);
+    uint64_t key;
+    if (cnb[s] == 0 || cnb[t] == 0) {
+      key = kKeyEmpty;
+    } else {
+      const int delta = clevel[t] - clevel[s];
+      const double wt = cmax[3 * t] - cmin[3 * t], ws = cmax[3 * s] - cmin[3 * s];
+      const double half = 0.5 * fmin(wt, ws);
+      bool ok = delta > -32 && delta < 32;
+      long long D[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double r = (ccen[3 * t + d] - ccen[3 * s + d]) / half;
+        D[d] = llrint(r);
+        ok = ok && fabs(r - (double)D[d]) < 1e-3 && D[d] > -kOffBias && D[d] < kOffBias;
+      }
+      key = ok ? ((uint64_t)(delta + 32) << 42) | ((uint64_t)(D[2] + kOffBias) << 28) |
+                     ((uint64_t)(D[1] + kOffBias) << 14) | (uint64_t)(D[0] + kOffBias)
+               : kKeyRare;
+    }
+    keys[e] = key;
+    vals[e] = (uint32_t)e;
+  }
+}
+
+__global__ void segment_flags(const uint64_t *__restrict__ keys, int64_t n,
+                              int32_t *__restrict__ flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// seg_start[c] = first sorted index of class c (c = scan value at a boundary)
+__global__ void segment_starts(const int32_t *__restrict__ flag, const int32_t *__restrict__ scan,
+                               int64_t n, int32_t *__restrict__ seg_start) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (flag[i]) seg_start[scan[i]] = (int32_t)i;
+}
+
+// per class: is it a tensor-core class?
+__global__ void class_tc_flags(const int32_t *__restrict__ seg_start, int64_t nseg, int64_t n,
+                               const uint64_t *__restrict__ keys, int32_t *__restrict__ tcflag,
+                               int32_t *__restrict__ ntiles) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
+    const uint64_t k = keys[b];
+    const bool tc = (k != kKeyEmpty) && (k != kKeyRare) && (e - b) >= kTcMin;
+    tcflag[c] = tc ? 1 : 0;
+    ntiles[c] = tc ? (int32_t)((e - b + kNTile - 1) / kNTile) : 0;
+  }
+}
+
+// Pairs of non-tensor-core classes (except empty-source pairs) go to FP64.
+__global__ void mark_fp64_pairs(const int32_t *__restrict__ seg_scan_incl_flag,
+                                const int32_t *__restrict__ scan, const int32_t *__restrict__ flag,
+                                const int32_t *__restrict__ tcflag,
+                                const uint64_t *__restrict__ keys,
+                                const uint32_t *__restrict__ vals, int64_t n,
+                                uint8_t *__restrict__ use64) {
+  (void)seg_scan_incl_flag;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int cls = scan[i] + flag[i] - 1;  // inclusive scan - 1
+    const bool empty = keys[i] == kKeyEmpty;
+    use64[vals[i]] = (!empty && !tcflag[cls]) ? 1 : 0;
+  }
+}
+
+struct TileItem {
+  int32_t cls;    // tensor-core class index (operator slot)
+  int32_t start;  // first sorted pair index
+  int32_t len;    // pairs in this tile (<= kNTile)
+  int32_t pad;
+};
+
+__global__ void build_tiles(const int32_t *__restrict__ seg_start, int64_t nseg, int64_t n,
+                            const int32_t *__restrict__ tcflag, const int32_t *__restrict__ tcid,
+                            const int32_t *__restrict__ tile_off,
+                            const uint64_t *__restrict__ keys, uint64_t *__restrict__ tc_keys,
+                            TileItem *__restrict__ items, int *__restrict__ tc_pairs) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (!tcflag[c]) continue;
+    const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
+    const int id = tcid[c];
+    tc_keys[id] = keys[b];
+    atomicAdd(tc_pairs, (int)(e - b));
+    int64_t o = tile_off[c];
+    for (int64_t p = b; p < e; p += kNTile, o++) {
+      TileItem it;
+      it.cls = id;
+      it.start = (int32_t)p;
+      it.len = (int32_t)min((int64_t)kNTile, e - p);
+      it.pad = 0;
+      items[o] = it;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+template <int P>
+__device__ __forceinline__ size_t op_offset(int r, int c) {
+  using S = TcShape<P>;
+  return ((size_t)(c / S::KC) * (S::MP / 8) + (size_t)(r / 8)) * (S::KC / 4 * 32) +
+         (size_t)((c % S::KC) / 4) * 32 + (size_t)(r % 8) * 4 + (size_t)(c % 4);
+}
+
+// One block per tensor-core class: unit-offset singular harmonics (evalLocal,
+// :102-135) in FP64, then every real operator entry, split hi/lo.
+template <int P>
+__global__ void __launch_bounds__(256) build_operators(const uint64_t *__restrict__ tc_keys,
+                                                       float *__restrict__ ops_hi,
+                                                       float *__restrict__ ops_lo) {
+  using S = TcShape<P>;
+  __shared__ cd Y[P * P];
+  const int cls = blockIdx.x;
+  const uint64_t key = tc_keys[cls];
+  const int delta = (int)((key >> 42) & 63) - 32;
+  const double Dx = (double)((long long)(key & 16383) - kOffBias);
+  const double Dy = (double)((long long)((key >> 14) & 16383) - kOffBias);
+  const double Dz = (double)((long long)((key >> 28) & 16383) - kOffBias);
+  // offset in units of the target width: D * 2^(min(delta,0) - 1)
+  const double u = ldexp(1.0, min(delta, 0) - 1);
+  double rho, alpha, beta;
+  cart2sph(Dx * u, Dy * u, Dz * u, rho, alpha, beta);
+  const double x = cos(alpha), y = sin(alpha);
+  double sb, cb;
+  sincos(beta, &sb, &cb);
+  if (threadIdx.x < P) local_column<P>(threadIdx.x, rho, x, y, cd{cb, sb}, Y);
+  __syncthreads();
+  float *hi = ops_hi + (size_t)cls * S::MP * S::KP;
+  float *lo = ops_lo + (size_t)cls * S::MP * S::KP;
+  for (int idx = threadIdx.x; idx < S::MP * S::KP; idx += blockDim.x) {
+    const int r = idx / S::KP, c = idx % S::KP;
+    double val = 0;
+    if (r < S::K && c < S::K) {
+      const int to = r >> 1, ti = c >> 1;  // complex output / input coefficient
+      const bool rim = r & 1, cim = c & 1;
+      int j, k, n, ma;
+      jk_of(to, j, k);
+      jk_of(ti, n, ma);
+      if (n < P - j) {
+        const double Cnm = oddeven(j);
+        const int base = (j + n) * (j + n) + j + n - k;
+        // m = +ma term: M * Cnm2 * Y[j+n, ma-k]
+        {
+          const double C2 = Cnm * oddeven((k - ma) * (k < ma) + ma);
+          const cd Yv = Y[base + ma];
+          const double cc = Yv.x, dd = Yv.y;
+          if (!rim && !cim) val += C2 * cc;
+          else if (!rim && cim) val += -C2 * dd;
+          else if (rim && !cim) val += C2 * dd;
+          else val += C2 * cc;
+        }
+        // m = -ma term (ma > 0): conj(M) * Cnm * Y[j+n, -ma-k]
+        if (ma > 0) {
+          const cd Yv = Y[base - ma];
+          const double cc = Yv.x, dd = Yv.y;
+          if (!rim && !cim) val += Cnm * cc;
+          else if (!rim && cim) val += Cnm * dd;
+          else if (rim && !cim) val += Cnm * dd;
+          else val += -Cnm * cc;
+        }
+        val = ldexp(val, delta * n);  // (w_s / w_t)^n
+      }
+    }
+    const float f = (float)val;
+    const float h = tf32_round(f);
+    const float l = tf32_round(f - h);
+    const size_t o = op_offset<P>(r, c);
+    hi[o] = h;
+    lo[o] = l;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// normalised FP32 multipoles and the final rescale into FP64 L
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
+                            const double *__restrict__ cmin, const double *__restrict__ cmax,
+                            const double2 *__restrict__ M, float *__restrict__ Mt) {
+  using S = TcShape<P>;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells * S::KP;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / S::KP;
+    const int kk = (int)(i % S::KP);
+    float v = 0.f;
+    if (kk < S::K && cnb[c] > 0) {
+      int n, m;
+      jk_of(kk >> 1, n, m);
+      const double w = cmax[3 * c] - cmin[3 * c];
+      const double2 z = M[c * S::NT + (kk >> 1)];
+      v = (float)(((kk & 1) ? z.y : z.x) * pow(w, -n));
+    }
+    Mt[i] = v;
+  }
+}
+
+template <int P>
+__global__ void add_scaled_L(int64_t ncells, const int32_t *__restrict__ cnb,
+                             const double *__restrict__ cmin, const double *__restrict__ cmax,
+                             const float *__restrict__ Lt, double2 *__restrict__ L) {
+  using S = TcShape<P>;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells * S::NT;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / S::NT;
+    const int t = (int)(i % S::NT);
+    if (cnb[c] == 0) continue;
+    int j, k;
+    jk_of(t, j, k);
+    const double w = cmax[3 * c] - cmin[3 * c];
+    const double sc = pow(w, -(j + 1));
+    const double2 o = L[i];
+    L[i] = make_double2(o.x + (double)Lt[c * S::KP + 2 * t] * sc,
+                        o.y + (double)Lt[c * S::KP + 2 * t + 1] * sc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers (inline PTX)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait (about 2 s of SM clock); false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > 4000000000LL) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  // base offset 0, absolute LBO mode, SWIZZLE_NONE (layout type 0)
+  return d;
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z),
+        "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+        "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// the GEMM kernel
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
+    const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
+    const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
+    const float *__restrict__ ops_lo, const float *__restrict__ Mt, float *__restrict__ Lt,
+    int *__restrict__ err) {
+  using S = TcShape<P>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned stage buffers
+  float *base = reinterpret_cast<float *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  float *stage[2];
+  stage[0] = base;
+  stage[1] = base + S::STAGE_FLOATS;
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int32_t pt[kNTile], ps[kNTile];
+  __shared__ int abort_sh;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint64_t mask = (1ull << shift) - 1;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"((uint32_t)S::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
+                         ((uint32_t)(128 >> 4) << 24);
+  const uint32_t LBO = 128;                  // adjacent k-cores
+  const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
+  uint32_t phase[2] = {0, 0};
+  bool pending[2] = {false, false};
+  bool failed = false;
+
+  for (int64_t it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
+    const TileItem item = items[it];
+    for (int i = tid; i < kNTile; i += blockDim.x) {
+      if (i < item.len) {
+        const uint64_t v = list[sorted_vals[item.start + i]];
+        pt[i] = (int)(v >> shift);
+        ps[i] = (int)(v & mask);
+      } else {
+        pt[i] = -1;
+        ps[i] = -1;
+      }
+    }
+    __syncthreads();
+    const float *ahi = ops_hi + (size_t)item.cls * S::MP * S::KP;
+    const float *alo = ops_lo + (size_t)item.cls * S::MP * S::KP;
+    for (int kc = 0; kc < S::NKC; kc++) {
+      const int b = kc & 1;
+      // the MMAs that last read this stage must be done
+      if (pending[b]) {
+        if (!mbar_wait_bounded(&bars[b], phase[b])) failed = true;
+        phase[b] ^= 1;
+        pending[b] = false;
+      }
+      float *sA_hi = stage[b];
+      float *sA_lo = sA_hi + S::MP * S::KC;
+      float *sB_hi = sA_lo + S::MP * S::KC;
+      float *sB_lo = sB_hi + kNTile * S::KC;
+      // A chunk: contiguous copy of the pre-laid-out operator chunk
+      {
+        const float4 *gh = reinterpret_cast<const float4 *>(ahi + (size_t)kc * S::MP * S::KC);
+        const float4 *gl = reinterpret_cast<const float4 *>(alo + (size_t)kc * S::MP * S::KC);
+        float4 *dh = reinterpret_cast<float4 *>(sA_hi);
+        float4 *dl = reinterpret_cast<float4 *>(sA_lo);
+        for (int i = tid; i < S::MP * S::KC / 4; i += blockDim.x) {
+          dh[i] = __ldg(gh + i);
+          dl[i] = __ldg(gl + i);
+        }
+      }
+      // B chunk: gather the sources' normalised multipoles, split hi/lo
+      for (int i = tid; i < kNTile * (S::KC / 4); i += blockDim.x) {
+        const int p = i / (S::KC / 4), cc = i % (S::KC / 4);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int s = ps[p];
+        if (s >= 0)
+          v = __ldg(reinterpret_cast<const float4 *>(Mt + (size_t)s * S::KP + kc * S::KC) + cc);
+        float4 h, l;
+        h.x = tf32_round(v.x); l.x = tf32_round(v.x - h.x);
+        h.y = tf32_round(v.y); l.y = tf32_round(v.y - h.y);
+        h.z = tf32_round(v.z); l.z = tf32_round(v.z - h.z);
+        h.w = tf32_round(v.w); l.w = tf32_round(v.w - h.w);
+        const int o = ((p >> 3) * (S::KC / 4) + cc) * 32 + (p & 7) * 4;
+        *reinterpret_cast<float4 *>(sB_hi + o) = h;
+        *reinterpret_cast<float4 *>(sB_lo + o) = l;
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0 && !failed) {
+        tc_fence_after();
+        const uint32_t a_hi = smem_u32(sA_hi), a_lo = smem_u32(sA_lo);
+        const uint32_t b_hi = smem_u32(sB_hi), b_lo = smem_u32(sB_lo);
+#pragma unroll
+        for (int mt = 0; mt < S::MT; mt++) {
+          const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
+          const uint32_t d = tmem + (uint32_t)(mt * kNTile);
+#pragma unroll
+          for (int s = 0; s < S::KC / 8; s++) {
+            const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
+            const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
+            const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
+            const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
+            const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
+            const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
+            umma_tf32(d, ah, bh, idesc, acc);
+            umma_tf32(d, al, bh, idesc, 1u);
+            umma_tf32(d, ah, bl, idesc, 1u);
+          }
+        }
+        umma_commit(&bars[b]);
+      }
+      pending[b] = true;
+    }
+    // all MMAs of the tile done
+    for (int b = 0; b < 2; b++) {
+      if (pending[b]) {
+        if (!mbar_wait_bounded(&bars[b], phase[b])) failed = true;
+        phase[b] ^= 1;
+        pending[b] = false;
+      }
+    }
+    if (failed) {
+      atomicExch(err, 1);
+      abort_sh = 1;
+    }
+    tc_fence_after();
+    __syncthreads();
+    if (abort_sh) break;
+    // epilogue: warp w reads TMEM lanes 32*(w%4).., columns of half (w/4)
+    {
+      const int q = warp & 3, h = warp >> 2;
+#pragma unroll 1
+      for (int mt = 0; mt < S::MT; mt++) {
+        const int r = mt * 128 + q * 32 + lane;
+#pragma unroll 1
+        for (int cchunk = 0; cchunk < 2; cchunk++) {
+          const int col0 = h * 64 + cchunk * 32;
+          uint32_t v[32];
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(mt * kNTile + col0);
+          tmem_ld32(taddr, v);
+          if (r < S::K) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const int t = pt[col0 + j];
+              if (t >= 0) atomicAdd(Lt + (size_t)t * S::KP + r, __uint_as_float(v[j]));
+            }
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"((uint32_t)S::TMEM_COLS)
+                 : "memory");
+  }
+}
+
+template <int P>
+int m2l_tc_P(tapas_b200_ctx *ctx) {
+  using S = TcShape<P>;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  const int64_t n = ctx->n_m2l;
+  auto &T = ctx->tc;
+  std::optional<PhaseTimer> setup_timer;
+  setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
+  // 1. classify + stable sort by class key
+  TB_CUDA(ctx, T.keys.ensure(n + 1, s));
+  TB_CUDA(ctx, T.keys_alt.ensure(n + 1, s));
+  TB_CUDA(ctx, T.vals.ensure(n + 1, s));
+  TB_CUDA(ctx, T.vals_alt.ensure(n + 1, s));
+  TB_CUDA(ctx, T.use64.ensure(n + 1, s));
+  if (n == 0) return TAPAS_B200_OK;
+  classify_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+      n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
+      ctx->ccen.p, T.keys.p, T.vals.p);
+  TB_LAUNCH_CHECK(ctx);
+  {
+    uint64_t *k = T.keys.p, *ka = T.keys_alt.p;
+    uint32_t *v = T.vals.p, *va = T.vals_alt.p;
+    TB_TRY(radix_sort(ctx, k, ka, v, va, n, 0, 48));
+    if (k != T.keys.p) { std::swap(T.keys.p, T.keys_alt.p); std::swap(T.keys.cap, T.keys_alt.cap); }
+    if (v != T.vals.p) { std::swap(T.vals.p, T.vals_alt.p); std::swap(T.vals.cap, T.vals_alt.cap); }
+  }
+  // 2. segments = classes
+  TB_CUDA(ctx, T.flag.ensure(n + 1, s));
+  TB_CUDA(ctx, T.scan.ensure(n + 1, s));
+  segment_flags<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.keys.p, n, T.flag.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_TRY(scan_exclusive(ctx, T.flag.p, T.scan.p, n, T.scan.p + n));
+  TB_CUDA(ctx, ctx->pinned.ensure(256));
+  int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, T.scan.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  const int64_t nseg = h[0];
+  TB_CUDA(ctx, T.seg_start.ensure(nseg + 1, s));
+  TB_CUDA(ctx, T.tcflag.ensure(nseg + 1, s));
+  TB_CUDA(ctx, T.tcid.ensure(nseg + 1, s));
+  TB_CUDA(ctx, T.ntiles.ensure(nseg + 1, s));
+  TB_CUDA(ctx, T.tile_off.ensure(nseg + 1, s));
+  segment_starts<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.flag.p, T.scan.p, n,
+                                                                    T.seg_start.p);
+  TB_LAUNCH_CHECK(ctx);
+  class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p,
+                                                      T.tcflag.p, T.ntiles.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_TRY(scan_exclusive(ctx, T.tcflag.p, T.tcid.p, nseg, T.tcid.p + nseg));
+  TB_TRY(scan_exclusive(ctx, T.ntiles.p, T.tile_off.p, nseg, T.tile_off.p + nseg));
+  mark_fp64_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+      nullptr, T.scan.p, T.flag.p, T.tcflag.p, T.keys.p, T.vals.p, n, T.use64.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, T.tcid.p + nseg, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaMemcpyAsync(h + 1, T.tile_off.p + nseg, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  const int64_t ntc = h[0], nitems = h[1];
+  ctx->tc_classes = ntc;
+  ctx->tc_tiles = nitems;
+  ctx->tc_segments = nseg;
+  // 3. operators
+  TB_CUDA(ctx, T.tc_keys.ensure(ntc + 1, s));
+  TB_CUDA(ctx, T.items.ensure((size_t)(nitems + 1) * sizeof(TileItem) / 16 + 1, s));
+  TB_CUDA(ctx, T.err.ensure(4, s));
+  TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
+  build_tiles<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.tcflag.p, T.tcid.p,
+                                                   T.tile_off.p, T.keys.p, T.tc_keys.p,
+                                                   reinterpret_cast<TileItem *>(T.items.p),
+                                                   T.err.p + 1);
+  TB_LAUNCH_CHECK(ctx);
+  const size_t opsz = (size_t)S::MP * S::KP;
+  if (ntc > 0) {
+    TB_CUDA(ctx, T.ops_hi.ensure(opsz * ntc, s));
+    TB_CUDA(ctx, T.ops_lo.ensure(opsz * ntc, s));
+    build_operators<P><<<(unsigned)ntc, 256, 0, s>>>(T.tc_keys.p, T.ops_hi.p, T.ops_lo.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  // 4. normalised multipoles, zeroed normalised locals
+  TB_CUDA(ctx, T.Mt.ensure((size_t)C * S::KP, s));
+  TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
+  normalize_M<P><<<grid_for(C * S::KP, 256, ctx->num_sms * 32), 256, 0, s>>>(
+      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
+  setup_timer.reset();
+  // 5. FP64 part (rare classes) writes L; the GEMM adds into Lt
+  TB_TRY(m2l_fp64_masked(ctx, T.use64.p));
+  if (nitems > 0) {
+    TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)S::SMEM));
+    const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
+    PhaseTimer t(ctx, &ctx->timings.m2l_tc);
+    m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(
+        reinterpret_cast<const TileItem *>(T.items.p), nitems, T.vals.p, ctx->m2l.p,
+        ctx->list_shift, T.ops_hi.p, T.ops_lo.p, T.Mt.p, T.Lt.p, T.err.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  add_scaled_L<P><<<grid_for(C * S::NT, 256, ctx->num_sms * 32), 256, 0, s>>>(
+      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, T.Lt.p, ctx->L.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->n_m2l_tc = h[1];
+  if (nitems > 0) {
+    if (h[0]) {
+      set_error(ctx, "m2l tensor-core kernel: a bounded wait on an MMA completion gave up");
+      return TAPAS_B200_ERR_TIMEOUT;
+    }
+  }
+  return TAPAS_B200_OK;
+}
+
+}  // namespace
+
+int m2l_tensorcore(tapas_b200_ctx *ctx) {
+  switch (ctx->P) {
+    case 4: return m2l_tc_P<4>(ctx);
+    case 5: return m2l_tc_P<5>(ctx);
+    case 6: return m2l_tc_P<6>(ctx);
+    case 7: return m2l_tc_P<7>(ctx);
+    case 8: return m2l_tc_P<8>(ctx);
+    case 9: return m2l_tc_P<9>(ctx);
+    case 10: return m2l_tc_P<10>(ctx);
+    case 11: return m2l_tc_P<11>(ctx);
+    case 12: return m2l_tc_P<12>(ctx);
+    case 13: return m2l_tc_P<13>(ctx);
+    case 14: return m2l_tc_P<14>(ctx);
+    case 15: return m2l_tc_P<15>(ctx);
+    case 16: return m2l_tc_P<16>(ctx);
+    default: break;
+  }
+  // P = 2, 3: too small for the tensor-core tiles; the FP64 kernel does all.
+  return m2l_fp64(ctx);
+}
+
+}  // namespace tb

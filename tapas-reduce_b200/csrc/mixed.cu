@@ -1,16 +1,18 @@
 // Mixed-precision evaluation path (TAPAS_B200_MIXED).
 //
-// Near field: FP32 compensated P2P (p2p.cu, p2p_mixed).  Far field: the
-// expansion passes keep their FP64 form; the near-field result is per unit
-// charge, so L2P adds to it without the reference's division by q_i.
+// Near field: FP32 compensated P2P (p2p.cu, p2p_mixed).  M2L: offset-class
+// batched split-TF32 GEMMs on the tensor cores (m2l_tc.cu).  Upward and
+// downward passes stay FP64; the near-field result is per unit charge, so
+// L2P adds to it without the reference's division by q_i.
 #include "kernels.cuh"
+#include "m2l_tc.cuh"
 #include "mixed.cuh"
 
 namespace tb {
 
 int upward_mixed(tapas_b200_ctx *ctx, int P) { return upward_fp64(ctx, P); }
 
-int m2l_mixed(tapas_b200_ctx *ctx) { return m2l_fp64(ctx); }
+int m2l_mixed(tapas_b200_ctx *ctx) { return m2l_tensorcore(ctx); }
 
 int downward_mixed(tapas_b200_ctx *ctx) { return downward_fp64(ctx); }
 
@@ -19,6 +21,15 @@ int mixed_sync_fp64_view(tapas_b200_ctx *ctx) {
   return TAPAS_B200_OK;
 }
 
-void mixed_release(tapas_b200_ctx *ctx) { ctx->rel4.release(); }
+void mixed_release(tapas_b200_ctx *ctx) {
+  ctx->rel4.release();
+  ctx->rel_lo.release();
+  ctx->p2p_wkey.release();
+  ctx->p2p_wkey_alt.release();
+  ctx->p2p_order.release();
+  ctx->p2p_order_alt.release();
+  ctx->p2p_counter.release();
+  ctx->tc.release();
+}
 
 }  // namespace tb

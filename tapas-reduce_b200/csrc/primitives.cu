@@ -90,6 +90,27 @@ __global__ void scan_total(const int32_t *in, const int32_t *out, int64_t n, int
 
 }  // namespace
 
+// Scan of in[0..n) into out using scratch[scratch_off..) for the block sums of
+// this level and the levels below (recursive reduce-then-scan).
+static int scan_level(tapas_b200_ctx *ctx, const int32_t *in, int32_t *out, int64_t n,
+                      size_t scratch_off) {
+  cudaStream_t s = ctx->stream;
+  const int64_t nb = (n + kScanTile - 1) / kScanTile;
+  if (nb == 1) {
+    scan_tiles<<<1, kScanThreads, 0, s>>>(in, out, n, nullptr);
+    TB_LAUNCH_CHECK(ctx);
+    return TAPAS_B200_OK;
+  }
+  int32_t *sums = ctx->scan_tmp.p + scratch_off;
+  int32_t *offs = sums + nb + 32;
+  scan_tiles<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums);
+  TB_LAUNCH_CHECK(ctx);
+  TB_TRY(scan_level(ctx, sums, offs, nb, scratch_off + 2 * (size_t)nb + 64));
+  scan_add<<<(unsigned)nb, kScanThreads, 0, s>>>(out, n, offs);
+  TB_LAUNCH_CHECK(ctx);
+  return TAPAS_B200_OK;
+}
+
 int scan_exclusive(tapas_b200_ctx *ctx, const int32_t *in, int32_t *out, int64_t n,
                    int32_t *d_total) {
   cudaStream_t s = ctx->stream;
@@ -97,27 +118,19 @@ int scan_exclusive(tapas_b200_ctx *ctx, const int32_t *in, int32_t *out, int64_t
     if (d_total) TB_CUDA(ctx, cudaMemsetAsync(d_total, 0, sizeof(int32_t), s));
     return TAPAS_B200_OK;
   }
-  const int64_t nb = (n + kScanTile - 1) / kScanTile;
-  if (nb == 1) {
-    scan_tiles<<<1, kScanThreads, 0, s>>>(in, out, n, nullptr);
-    TB_LAUNCH_CHECK(ctx);
-  } else {
-    // Block sums live after the caller-visible scratch region.
-    size_t need = (size_t)nb * 2 + 64;
-    TB_CUDA(ctx, ctx->scan_tmp.ensure(need, s));
-    int32_t *sums = ctx->scan_tmp.p;
-    int32_t *offs = ctx->scan_tmp.p + nb + 32;
-    scan_tiles<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums);
-    TB_LAUNCH_CHECK(ctx);
-    if (nb > kScanTile) {
-      set_error(ctx, "scan: %lld elements exceed the two-level scan limit", (long long)n);
-      return TAPAS_B200_ERR_CAPACITY;
-    }
-    scan_tiles<<<1, kScanThreads, 0, s>>>(sums, offs, nb, nullptr);
-    TB_LAUNCH_CHECK(ctx);
-    scan_add<<<(unsigned)nb, kScanThreads, 0, s>>>(out, n, offs);
-    TB_LAUNCH_CHECK(ctx);
+  if (n > (int64_t)0x7FFFFFFF) {
+    set_error(ctx, "scan: %lld elements exceed int32 offsets", (long long)n);
+    return TAPAS_B200_ERR_CAPACITY;
   }
+  // scratch for every level: sum over levels of 2 * blocks + 64
+  size_t need = 64;
+  for (int64_t m = n; m > kScanTile;) {
+    const int64_t nb = (m + kScanTile - 1) / kScanTile;
+    need += 2 * (size_t)nb + 64;
+    m = nb;
+  }
+  TB_CUDA(ctx, ctx->scan_tmp.ensure(need, s));
+  TB_TRY(scan_level(ctx, in, out, n, 0));
   if (d_total) {
     scan_total<<<1, 32, 0, s>>>(in, out, n, d_total);
     TB_LAUNCH_CHECK(ctx);

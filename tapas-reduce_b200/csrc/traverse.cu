@@ -68,17 +68,24 @@ __global__ void __launch_bounds__(kBlock) dtt_step(CellView c, double theta,
                                                    int2 *__restrict__ next, int64_t next_cap,
                                                    uint64_t *__restrict__ m2l, int64_t m2l_cap,
                                                    uint64_t *__restrict__ p2p, int64_t p2p_cap,
-                                                   unsigned long long *__restrict__ counters) {
+                                                   unsigned long long *__restrict__ counters,
+                                                   int prune_empty) {
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nfront;
        base += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = base + threadIdx.x;
     int kind = 0;  // 0 none, 1 m2l, 2 p2p, 3 split target, 4 split source
     int t = 0, s = 0;
     unsigned long long inter = 0;
-    if (i < nfront) {
+    bool live = i < nfront;
+    if (live) {
       int2 pr = front[i];
       t = pr.x;
       s = pr.y;
+      // An empty cell (and so all of its descendants) contributes nothing as a
+      // source and receives nothing used later as a target.
+      if (prune_empty && (c.nb[t] == 0 || c.nb[s] == 0)) live = false;
+    }
+    if (live) {
       const double dx = __dsub_rn(c.cen[3 * t + 0], c.cen[3 * s + 0]);
       const double dy = __dsub_rn(c.cen[3 * t + 1], c.cen[3 * s + 1]);
       const double dz = __dsub_rn(c.cen[3 * t + 2], c.cen[3 * s + 2]);
@@ -207,7 +214,8 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
       TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s));
       dtt_step<<<grid_for(nfront, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
           cv, theta, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
-          (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p);
+          (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p,
+          ctx->reference_lists ? 0 : 1);
       TB_LAUNCH_CHECK(ctx);
       TB_CUDA(ctx, cudaMemcpyAsync(hc, ctx->counters.p, 5 * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s));

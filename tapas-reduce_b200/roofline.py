@@ -28,8 +28,8 @@ def nominal_tflops(kind: str, sm_mhz: float, sms: int = 148) -> float:
 def dominant(phases: dict, lists: dict, tree: dict, P: int, peaks: dict, peak_src: str,
              precision: str = "mixed") -> dict:
     cand = {k: phases.get(k, 0.0) for k in ("bbox_keys", "sort", "tree", "p2m", "m2m",
-                                            "traverse", "list_sort", "m2l", "p2p", "l2l",
-                                            "l2p")}
+                                            "traverse", "list_sort", "m2l_setup", "m2l_fp64",
+                                            "m2l_tc", "p2p", "l2l", "l2p")}
     name = max(cand, key=cand.get)
     ms = cand[name]
     smx = float(peaks.get("sm_max_mhz", 1965.0))
@@ -37,6 +37,25 @@ def dominant(phases: dict, lists: dict, tree: dict, P: int, peaks: dict, peak_sr
     if ms <= 0:
         return out
     n = tree.get("n_bodies", 0)
+    if name == "m2l_tc":
+        # tensor pipe: TF32 dense peak = half the measured bf16 dense peak
+        ntc = lists.get("n_m2l_tc", 0)
+        fl = float(m2l_flops_per_translation(P)) * ntc
+        K = P * (P + 1)
+        mp = ((K + 127) // 128) * 128
+        kc = 32 if mp <= 256 else 16
+        kp = ((K + kc - 1) // kc) * kc
+        executed = float(lists.get("tc_tiles", 0)) * 128 * mp * kp * 2 * 3
+        peak = float(peaks.get("bf16_tflops", 1590.0)) / 2
+        ach = fl / (ms * 1e-3) / 1e12
+        out.update(bound="tensor", achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
+                   peak_source=f"TF32 dense = bf16 {peak_src} / 2", traffic=None,
+                   executed_mma_tflops=executed / (ms * 1e-3) / 1e12,
+                   work=f"{ntc} translations x {m2l_flops_per_translation(P)} flop "
+                        f"(algorithmic); MMA executes 3 x 2 x 128 x {mp} x {kp} per tile")
+        return out
+    if name == "m2l_fp64":
+        name = "m2l"
     if name == "p2p":
         fl = 20.0 * lists["n_p2p_interactions"]
         kind = "fp32" if precision == "mixed" else "fp64"

@@ -52,8 +52,15 @@ def run(request, tb, oracle_mod, ctx):
     o = oracle_mod.Oracle(x, y, z, q, P=P, ncrit=ncrit, theta=theta)
     ctx.partition(x, y, z, q, ncrit=ncrit)
     ctx.upward(P, tb.FP64)
+    # lists exactly as the reference's traversal visits them ...
+    ctx.set_reference_lists(True)
     ctx.build_lists(theta)
     lists = ctx.lists()
+    linfo = ctx.list_info()
+    # ... and the default lists without pairs of empty cells, used for the results
+    ctx.set_reference_lists(False)
+    ctx.build_lists(theta)
+    pruned = ctx.lists()
     ctx.m2l(tb.FP64)
     ctx.p2p(tb.FP64)
     ctx.downward(tb.FP64)
@@ -63,7 +70,7 @@ def run(request, tb, oracle_mod, ctx):
     M, L = ctx.expansions()
     return dict(x=x, y=y, z=z, q=q, P=P, theta=theta, o=o, res=res, cells=cells, lists=lists,
                 sorted_idx=sorted_idx, sorted_keys=sorted_keys, M=M, L=L,
-                info=ctx.tree_info(), linfo=ctx.list_info())
+                info=ctx.tree_info(), linfo=linfo, pruned=pruned)
 
 
 def test_tree_bit_exact(run):
@@ -105,6 +112,16 @@ def test_lists_equal_as_sets(run):
     assert np.all(np.diff(packed) > 0)
 
 
+def test_pruned_lists_drop_only_empty_pairs(run):
+    """Default lists = reference lists minus the pairs with an empty cell."""
+    gkeys, nb = run["cells"]["key"], run["cells"]["nb"]
+    (rmt, rms), (rpt, rps) = run["lists"]
+    (pmt, pms), (ppt, pps) = run["pruned"]
+    keep = (nb[rmt] > 0) & (nb[rms] > 0)
+    assert _pair_keys(gkeys, pmt, pms) == _pair_keys(gkeys, rmt[keep], rms[keep])
+    assert _pair_keys(gkeys, ppt, pps) == _pair_keys(gkeys, rpt, rps)
+
+
 def test_expansions_fp64(run):
     o = run["o"]
     oM, oL = o.expansions()
@@ -128,8 +145,12 @@ def test_results_fp64(run):
 def test_against_reference_goldens(path, tb, ctx):
     """Directly against outputs of the unmodified reference."""
     g = np.load(path)
-    res = ctx.evaluate(g["x"], g["y"], g["z"], g["q"], P=int(g["P"]), ncrit=int(g["ncrit"]),
-                       theta=float(g["theta"]), precision=tb.FP64)
+    ctx.set_reference_lists(True)
+    try:
+        res = ctx.evaluate(g["x"], g["y"], g["z"], g["q"], P=int(g["P"]), ncrit=int(g["ncrit"]),
+                           theta=float(g["theta"]), precision=tb.FP64)
+    finally:
+        ctx.set_reference_lists(False)
     c = ctx.cells()
     order = np.argsort(c["key"], kind="stable")
     assert np.array_equal(c["key"][order], g["cell_key"])
@@ -159,6 +180,25 @@ def test_mixed_close_to_fp64(tb, ctx, oracle_mod):
     assert emx[0] < 1.5 * e64[0] + 1e-6 and emx[1] < 1.5 * e64[1] + 1e-6
 
 
+@pytest.mark.parametrize("P", [4, 6, 8, 10, 11, 12, 14, 16])
+def test_tensorcore_m2l_matches_fp64(P, tb, ctx):
+    """Split-TF32 tensor-core M2L (mixed) against the FP64 M2L: per cell,
+    ||L_mixed - L_fp64|| / ||L_fp64|| <= 2e-5 (FP32 accumulation of ~100-300
+    translations of ~1e-7 relative accuracy each)."""
+    x, y, z, q = tb.datasets.make("plummer", 60000, 61)
+    ctx.partition(x, y, z, q, ncrit=32)
+    ctx.upward(P, tb.FP64)
+    ctx.build_lists(0.4)
+    ctx.m2l(tb.FP64)
+    _, L64 = ctx.expansions()
+    ctx.m2l(tb.MIXED)
+    _, Lmx = ctx.expansions()
+    nb = ctx.cells()["nb"]
+    ne = (nb > 0) & (np.linalg.norm(L64, axis=1) > 0)
+    rel = np.linalg.norm(Lmx[ne] - L64[ne], axis=1) / np.linalg.norm(L64[ne], axis=1)
+    assert rel.max() < 2e-5, (rel.max(), np.median(rel))
+
+
 def test_gpu_direct_matches_oracle_direct(tb, ctx, oracle_mod):
     x, y, z, q = tb.datasets.make("uniform_cube", 20000, 3)
     ctx.partition(x, y, z, q, ncrit=64)
@@ -179,11 +219,17 @@ def test_fp64_accuracy_vs_direct(tb, ctx, oracle_mod):
 
 
 def test_deterministic(tb, ctx):
+    """The FP64 form is bit-reproducible (lists sorted, no atomics).  The mixed
+    form adds tensor-core M2L columns into FP32 locals with atomic reductions,
+    so the summation order, and the last bits, vary between runs: repeat runs
+    agree to 1e-7 relative."""
     x, y, z, q = tb.datasets.make("plummer", 30000, 23)
-    for prec in (tb.FP64, tb.MIXED):
-        a = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=prec)
-        b = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=prec)
-        assert np.array_equal(a, b)
+    a = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=tb.FP64)
+    b = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=tb.FP64)
+    assert np.array_equal(a, b)
+    a = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=tb.MIXED)
+    b = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=0.4, precision=tb.MIXED)
+    assert _rel(a, b) < 1e-7
 
 
 @pytest.mark.parametrize("n,ncrit", [(1, 64), (2, 1), (5, 2), (50, 64), (64, 64), (65, 64)])
