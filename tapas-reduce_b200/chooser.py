@@ -16,7 +16,7 @@ _FP64_P_BY_TOL = [(1e-4, 8), (2e-5, 10), (5e-6, 12), (1.5e-6, 14), (0.0, 16)]
 # mixed form before the learned chooser: the cheapest measured setting per tolerance
 _MIXED_TABLE = [(1e-4, {"P": 8, "theta": 0.4, "ncrit": 64}),
                 (2e-5, {"P": 10, "theta": 0.4, "ncrit": 64}),
-                (0.0, {"P": 12, "theta": 0.3, "ncrit": 64})]
+                (0.0, {"P": 10, "theta": 0.3, "ncrit": 64})]
 
 
 def choose_params(n: int, tol: float, precision: str = "mixed", features=None) -> dict:
