@@ -181,6 +181,26 @@ int tapas_b200_evaluate(tapas_b200_ctx *ctx, const double *x, const double *y, c
 int tapas_b200_direct(tapas_b200_ctx *ctx, const int64_t *targets, int64_t k, double *out4,
                       int mem);
 
+/* The same FP64 direct-sum check, for callers that must not allocate device
+ * memory at the point where they verify accuracy: a solver loop that reserved
+ * all of its device memory up front, or code sharing the GPU with other
+ * streams (cudaMalloc/cudaFree synchronise the whole device).  This entry
+ * point has no counterpart in the reference.
+ *  - x, y, z, q (n bodies), targets (k original indices) and out4 (4*k) are
+ *    caller-owned DEVICE buffers on the current device; work goes on `stream`
+ *    (a cudaStream_t, NULL = default stream) and is not synchronised.
+ *  - It allocates nothing: partial sums live in one fixed 2 MiB device array
+ *    built into the library, present once on every GPU that loads it until
+ *    the process exits.  At most 4096 targets per call; larger k returns
+ *    TAPAS_B200_ERR_CAPACITY.  A target index outside [0, n) gives NaN.
+ *  - Calls share that array and it keeps the last call's contents: calls
+ *    that overlap on the GPU race and must be serialised by the caller.
+ *  - The first call on a device looks up the array's address; make it before
+ *    any stream capture.  Errors: tapas_b200_last_error(NULL). */
+int tapas_b200_direct_noalloc(const double *x, const double *y, const double *z, const double *q,
+                              int64_t n, const int64_t *targets, int64_t k, double *out4,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif
