@@ -130,6 +130,32 @@ int tapas_b200_get_cells(tapas_b200_ctx *ctx, uint64_t *key, int32_t *leaf, int3
                          double *width3);
 /* Sorted bodies: original index and Morton key per sorted position. Host memory. */
 int tapas_b200_get_sorted(tapas_b200_ctx *ctx, int64_t *orig_index, uint64_t *keys);
+/* Number of bodies per leaf depth of the current tree (leaves deeper than
+ * nbins-1 count in the last bin); nbins in 1..64; hist = nbins host int64.
+ * The octree-shape feature of the learned parameter chooser (the reference
+ * prints the same per-depth leaf histogram under TAPAS_DEBUG_HISTOGRAM,
+ * hot/buildtree.h:89-117). */
+int tapas_b200_leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *hist);
+
+/* ---- learned parameter chooser: network trained and run by own kernels ---- */
+/* No counterpart in the reference (the learned part of this implementation).
+ * Fully connected n_in -> n_hidden x n_layers (tanh) -> n_out (linear), FP32,
+ * parameters one flat array (per layer W out x in row-major, then b). */
+int tapas_b200_mlp_create(tapas_b200_ctx *ctx, int n_in, int n_hidden, int n_layers, int n_out,
+                          uint64_t seed);
+int64_t tapas_b200_mlp_num_params(tapas_b200_ctx *ctx);
+int tapas_b200_mlp_set_params(tapas_b200_ctx *ctx, const float *params);
+int tapas_b200_mlp_get_params(tapas_b200_ctx *ctx, float *params);
+/* Y[n x n_out] = net(X[n x n_in]); host arrays. */
+int tapas_b200_mlp_forward(tapas_b200_ctx *ctx, const float *X, int64_t n, float *Y);
+/* Gradient of the mean squared error over the n samples w.r.t. all
+ * parameters (flat layout) and the loss; host arrays. */
+int tapas_b200_mlp_gradients(tapas_b200_ctx *ctx, const float *X, const float *Y, int64_t n,
+                             float *grads, float *loss);
+/* Adam training, minibatches of `batch` samples in a seeded shuffle order;
+ * loss_per_epoch (may be NULL) gets the mean loss of each epoch. */
+int tapas_b200_mlp_train(tapas_b200_ctx *ctx, const float *X, const float *Y, int64_t n,
+                         int epochs, int batch, float lr, uint64_t seed, float *loss_per_epoch);
 
 /* ---- evaluation ---------------------------------------------------------- */
 

@@ -29,7 +29,10 @@ EXPORTS = (
     "tapas_b200_traverse", "tapas_b200_build_lists", "tapas_b200_list_info",
     "tapas_b200_get_lists", "tapas_b200_m2l", "tapas_b200_p2p", "tapas_b200_downward",
     "tapas_b200_get_expansions", "tapas_b200_get_results", "tapas_b200_evaluate",
-    "tapas_b200_direct",
+    "tapas_b200_direct", "tapas_b200_direct_noalloc", "tapas_b200_leaf_depth_histogram",
+    "tapas_b200_mlp_create", "tapas_b200_mlp_num_params", "tapas_b200_mlp_set_params",
+    "tapas_b200_mlp_get_params", "tapas_b200_mlp_forward", "tapas_b200_mlp_gradients",
+    "tapas_b200_mlp_train",
 )
 
 
@@ -106,6 +109,23 @@ def lib():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = _int
+    sig2 = {
+        "tapas_b200_leaf_depth_histogram": [_vp, _int, _vp],
+        "tapas_b200_mlp_create": [_vp, _int, _int, _int, _int, ctypes.c_uint64],
+        "tapas_b200_mlp_set_params": [_vp, _vp],
+        "tapas_b200_mlp_get_params": [_vp, _vp],
+        "tapas_b200_mlp_forward": [_vp, _vp, _i64, _vp],
+        "tapas_b200_mlp_gradients": [_vp, _vp, _vp, _i64, _vp, _vp],
+        "tapas_b200_mlp_train": [_vp, _vp, _vp, _i64, _int, _int, ctypes.c_float,
+                                 ctypes.c_uint64, _vp],
+        "tapas_b200_direct_noalloc": [_vp] * 4 + [_i64, _vp, _i64, _vp, _vp],
+    }
+    for name, args in sig2.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = _int
+    L.tapas_b200_mlp_num_params.argtypes = [_vp]
+    L.tapas_b200_mlp_num_params.restype = _i64
     L.tapas_b200_last_error.argtypes = [_vp]
     L.tapas_b200_last_error.restype = ctypes.c_char_p
     L.tapas_b200_kernel_launches.argtypes = [_vp, _int]
@@ -285,6 +305,54 @@ class Context:
                                                 float(theta), precision, op, order, mem))
         self.n = n
         return out
+
+    def leaf_depth_histogram(self, nbins: int = 16) -> np.ndarray:
+        h = np.zeros(nbins, np.int64)
+        self._check(self._L.tapas_b200_leaf_depth_histogram(self.h, nbins,
+                                                            h.ctypes.data_as(_vp)))
+        return h
+
+    # ---- learned-chooser network (own CUDA kernels) -----------------------
+    def mlp_create(self, n_in, n_hidden=64, n_layers=3, n_out=2, seed=0):
+        self._check(self._L.tapas_b200_mlp_create(self.h, n_in, n_hidden, n_layers, n_out,
+                                                  seed))
+        return int(self._L.tapas_b200_mlp_num_params(self.h))
+
+    def mlp_params(self) -> np.ndarray:
+        p = np.zeros(int(self._L.tapas_b200_mlp_num_params(self.h)), np.float32)
+        self._check(self._L.tapas_b200_mlp_get_params(self.h, p.ctypes.data_as(_vp)))
+        return p
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self._L.tapas_b200_mlp_set_params(self.h, p.ctypes.data_as(_vp)))
+
+    def mlp_forward(self, X, n_out=2) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.zeros((len(X), n_out), np.float32)
+        self._check(self._L.tapas_b200_mlp_forward(self.h, X.ctypes.data_as(_vp), len(X),
+                                                   Y.ctypes.data_as(_vp)))
+        return Y
+
+    def mlp_gradients(self, X, Y):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        g = np.zeros(int(self._L.tapas_b200_mlp_num_params(self.h)), np.float32)
+        loss = ctypes.c_float()
+        self._check(self._L.tapas_b200_mlp_gradients(self.h, X.ctypes.data_as(_vp),
+                                                     Y.ctypes.data_as(_vp), len(X),
+                                                     g.ctypes.data_as(_vp), ctypes.byref(loss)))
+        return g, float(loss.value)
+
+    def mlp_train(self, X, Y, epochs=200, batch=128, lr=1e-3, seed=0) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        hist = np.zeros(epochs, np.float32)
+        self._check(self._L.tapas_b200_mlp_train(self.h, X.ctypes.data_as(_vp),
+                                                 Y.ctypes.data_as(_vp), len(X), epochs, batch,
+                                                 ctypes.c_float(lr), seed,
+                                                 hist.ctypes.data_as(_vp)))
+        return hist
 
     def direct(self, targets) -> np.ndarray:
         tg = np.ascontiguousarray(targets, dtype=np.int64)

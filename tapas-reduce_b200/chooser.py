@@ -1,30 +1,180 @@
-"""Parameter choice (expansion order P, MAC theta, leaf size ncrit) for a
-requested relative-L2 potential tolerance.
+"""Parameter choice for a requested relative-L2 potential tolerance.
 
-``choose_params`` returns the setting a run should use and where it came
-from.  The plain FP64 form uses the reference's fixed theta = 0.4 and
-ncrit = 64 and raises P until the tolerance is met (measured on the
-sphere-surface workload: P=10 -> 1.6e-5, P=12 -> 4.0e-6, P=14 -> 1.3e-6,
-P=16 -> 7.5e-7).  The fixed fallback is the reference's default setting.
+Two ways to choose (expansion order P, MAC theta, leaf size ncrit and the
+arithmetic form, mixed or FP64):
+
+* the learned chooser: a 3 x 64 tanh network (csrc/mlp.cu, trained and run by
+  this library's own CUDA kernels) maps the system's features plus one
+  candidate setting to its predicted log10 potential error and log10 time.
+  All candidates of the grid (P 4..16, theta 0.20..0.70, ncrit 16/32/64/128,
+  mixed/FP64) are scored in one batched forward pass and the cheapest one
+  whose predicted error plus a safety margin is within the tolerance wins.
+  System features: log10 N, the fraction of bodies per leaf depth (16 bins)
+  of the tree built with ncrit = 64, and the net-charge ratio |sum q|/sum|q|
+  (zero-mean charges cancel and need more accuracy).
+* rules without learning: the plain FP64 form keeps the reference's
+  theta = 0.4 and ncrit = 64 and raises P until the tolerance is met
+  (measured on the sphere-surface workload: P=10 -> 1.6e-5, P=12 -> 4.0e-6,
+  P=14 -> 1.3e-6, P=16 -> 7.5e-7); the fixed fallback is P=10, theta=0.4,
+  ncrit=64, FP64 (the reference's default setting).
+
+``evaluate_verified`` runs the chosen setting, checks it against an FP64
+direct sum on sampled targets, and falls back to the fixed setting when the
+check misses the tolerance.
 """
 from __future__ import annotations
 
-FIXED = {"P": 10, "theta": 0.4, "ncrit": 64}
+import pathlib
 
-# (tol upper bound, P) for the plain form at theta=0.4, ncrit=64
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+MODEL_PATH = HERE / "chooser_model.npz"
+
+FIXED = {"P": 10, "theta": 0.4, "ncrit": 64, "precision": "fp64"}
+NBINS = 16
+FEATURE_NCRIT = 64
+
+P_GRID = np.arange(4, 17)
+THETA_GRID = np.round(np.arange(0.20, 0.7001, 0.05), 2)
+NCRIT_GRID = np.array([16, 32, 64, 128])
+PREC_GRID = np.array([0, 1])  # 0 mixed, 1 fp64
+
+# rules without learning
 _FP64_P_BY_TOL = [(1e-4, 8), (2e-5, 10), (5e-6, 12), (1.5e-6, 14), (0.0, 16)]
-# mixed form before the learned chooser: the cheapest measured setting per tolerance
 _MIXED_TABLE = [(1e-4, {"P": 8, "theta": 0.4, "ncrit": 64}),
                 (2e-5, {"P": 10, "theta": 0.4, "ncrit": 64}),
                 (0.0, {"P": 10, "theta": 0.3, "ncrit": 64})]
 
 
-def choose_params(n: int, tol: float, precision: str = "mixed", features=None) -> dict:
+# ---------------------------------------------------------------------------
+# features and encodings
+# ---------------------------------------------------------------------------
+def charge_ratio(q) -> float:
+    q = np.asarray(q, np.float64)
+    a = float(np.sum(np.abs(q)))
+    return float(abs(np.sum(q)) / a) if a > 0 else 1.0
+
+
+def system_features(ctx, x, y, z, q) -> np.ndarray:
+    """[log10 N, 16 leaf-depth fractions, net-charge ratio] of a body set.
+    Builds the ncrit = 64 tree on ctx (replacing its current tree)."""
+    n = len(x)
+    ctx.partition(x, y, z, q, ncrit=FEATURE_NCRIT)
+    h = ctx.leaf_depth_histogram(NBINS).astype(np.float64)
+    h = h / max(h.sum(), 1.0)
+    return np.concatenate([[np.log10(n)], h, [charge_ratio(q)]])
+
+
+def encode(features: np.ndarray, P, theta, ncrit, fp64) -> np.ndarray:
+    """Network input rows for one system and arrays of candidate settings."""
+    P = np.atleast_1d(np.asarray(P, np.float64))
+    k = len(P)
+    cand = np.stack([(P - 10.0) / 4.0,
+                     (np.asarray(theta, np.float64) - 0.45) / 0.15 * np.ones(k),
+                     np.log2(np.asarray(ncrit, np.float64)) - 6.0 * np.ones(k),
+                     np.asarray(fp64, np.float64) * np.ones(k)], axis=1)
+    return np.concatenate([np.repeat(features[None, :], k, axis=0), cand], axis=1)
+
+
+def candidate_grid():
+    g = np.array(np.meshgrid(P_GRID, THETA_GRID, NCRIT_GRID, PREC_GRID, indexing="ij"))
+    return g.reshape(4, -1).T  # rows: P, theta, ncrit, fp64
+
+
+# ---------------------------------------------------------------------------
+# the learned chooser
+# ---------------------------------------------------------------------------
+class LearnedChooser:
+    def __init__(self, ctx, model_path=MODEL_PATH):
+        m = np.load(model_path)
+        self.dims = [int(d) for d in m["dims"]]
+        self.params = m["params"].astype(np.float32)
+        self.x_mean, self.x_std = m["x_mean"], m["x_std"]
+        self.y_mean, self.y_std = m["y_mean"], m["y_std"]
+        self.margin = float(m["margin"])
+        self.ctx = ctx
+        ctx.mlp_create(self.dims[0], self.dims[1], len(self.dims) - 2, self.dims[-1], seed=0)
+        ctx.mlp_set_params(self.params)
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        Xs = ((X - self.x_mean) / self.x_std).astype(np.float32)
+        Y = self.ctx.mlp_forward(Xs, n_out=self.dims[-1]).astype(np.float64)
+        return Y * self.y_std + self.y_mean  # columns: log10 err, log10 time
+
+    def choose(self, features: np.ndarray, tol: float, precisions=(0, 1)) -> dict:
+        g = candidate_grid()
+        g = g[np.isin(g[:, 3], precisions)]
+        pred = self.predict(encode(features, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
+        ok = pred[:, 0] + self.margin <= np.log10(tol)
+        if ok.any():
+            idx = np.flatnonzero(ok)[np.argmin(pred[ok, 1])]
+            src = "learned"
+        else:  # nothing predicted to meet it: the most accurate candidate
+            idx = int(np.argmin(pred[:, 0]))
+            src = "learned-best-effort"
+        P, th, nc, f64 = g[idx]
+        return {"P": int(P), "theta": float(th), "ncrit": int(nc),
+                "precision": "fp64" if f64 else "mixed", "source": src,
+                "pred_log10_err": float(pred[idx, 0]), "pred_log10_ms": float(pred[idx, 1])}
+
+
+_cache = {}
+
+
+def learned_chooser(ctx):
+    if not MODEL_PATH.exists():
+        return None
+    key = id(ctx)
+    if key not in _cache:
+        _cache[key] = LearnedChooser(ctx)
+    return _cache[key]
+
+
+# ---------------------------------------------------------------------------
+# public entry points
+# ---------------------------------------------------------------------------
+def choose_params(n: int, tol: float, precision: str = "mixed", features=None,
+                  ctx=None) -> dict:
+    """Setting for a run.  With ctx and features and a trained model, the
+    learned chooser (restricted to `precision` unless "auto"); otherwise the
+    rules."""
+    if ctx is not None and features is not None:
+        lc = learned_chooser(ctx)
+        if lc is not None:
+            precs = {"mixed": (0,), "fp64": (1,), "auto": (0, 1)}[precision]
+            return lc.choose(features, tol, precs)
     if precision == "fp64":
         for bound, P in _FP64_P_BY_TOL:
             if tol >= bound:
-                return {"P": P, "theta": 0.4, "ncrit": 64, "source": "fixed-theta P rule"}
+                return {"P": P, "theta": 0.4, "ncrit": 64, "precision": "fp64",
+                        "source": "fixed-theta P rule"}
     for bound, prm in _MIXED_TABLE:
         if tol >= bound:
-            return dict(prm, source="table")
+            return dict(prm, precision="mixed", source="table")
     return dict(FIXED, source="fixed")
+
+
+def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=None):
+    """Chosen setting -> evaluation -> FP64 direct-sum check on `targets` ->
+    fixed fallback on a miss.  Returns (results, info)."""
+    from importlib import import_module
+    rel_l2 = import_module("tapas_reduce_b200.verify").rel_l2
+    if params is None:
+        if features is None:
+            features = system_features(ctx, x, y, z, q)
+        params = choose_params(len(x), tol, "auto", features=features, ctx=ctx)
+    prec = tb.FP64 if params["precision"] == "fp64" else tb.MIXED
+    res = ctx.evaluate(x, y, z, q, P=params["P"], ncrit=params["ncrit"], theta=params["theta"],
+                       precision=prec)
+    d = ctx.direct(targets)
+    err = rel_l2(res[targets], d)
+    info = {"params": params, "rel_l2_pot": err[0], "rel_l2_acc": err[1],
+            "met": err[0] <= tol, "fallback": False}
+    if not info["met"]:
+        res = ctx.evaluate(x, y, z, q, P=FIXED["P"], ncrit=FIXED["ncrit"], theta=FIXED["theta"],
+                           precision=tb.FP64)
+        err = rel_l2(res[targets], d)
+        info.update(fallback=True, fallback_rel_l2_pot=err[0], fallback_rel_l2_acc=err[1],
+                    fallback_met=err[0] <= tol)
+    return res, info

@@ -186,6 +186,7 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->M.release();
   ctx->L.release();
   mixed_release(ctx);
+  mlp_release(ctx);
   ctx->pinned.release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -307,6 +308,11 @@ int tapas_b200_get_cells(tapas_b200_ctx *ctx, uint64_t *key, int32_t *leaf, int3
   }
   TB_CUDA(ctx, cudaStreamSynchronize(s));
   return TAPAS_B200_OK;
+}
+
+int tapas_b200_leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *hist) {
+  TB_TRY(check_ctx(ctx));
+  return leaf_depth_histogram(ctx, nbins, hist);
 }
 
 int tapas_b200_get_sorted(tapas_b200_ctx *ctx, int64_t *orig_index, uint64_t *keys) {

@@ -98,6 +98,8 @@ struct HBuf {
   }
 };
 
+struct Mlp;  // learned-chooser network (mlp.cu)
+
 // Work state of the tensor-core M2L (m2l_tc.cu).
 struct TcState {
   DBuf<uint64_t> keys, keys_alt, tc_keys;
@@ -188,8 +190,14 @@ struct tapas_b200_ctx {
   bool have_M = false, have_L = false;
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
 
+  tb::Mlp *mlp = nullptr;               // learned chooser network, if created
+
   tb::HBuf pinned;
 };
+
+namespace tb {
+void mlp_release(tapas_b200_ctx *ctx);
+}
 
 namespace tb {
 

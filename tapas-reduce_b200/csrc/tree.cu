@@ -215,7 +215,42 @@ __global__ void compact_indices(const int32_t *__restrict__ flag,
     if (flag[i]) out[scan[i]] = (int32_t)i;
 }
 
+__global__ void leaf_depth_hist(const int32_t *__restrict__ leaves, int64_t nleaves,
+                                const int32_t *__restrict__ clevel, const int32_t *__restrict__ cnb,
+                                int nbins, unsigned long long *__restrict__ hist) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nleaves;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int c = leaves[w];
+    const int d = min(clevel[c], nbins - 1);
+    atomicAdd(hist + d, (unsigned long long)cnb[c]);
+  }
+}
+
 }  // namespace
+
+int leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *out) {
+  if (!ctx->have_tree) {
+    set_error(ctx, "leaf_depth_histogram: no tree");
+    return TAPAS_B200_ERR_STATE;
+  }
+  if (nbins < 1 || nbins > 64 || !out) {
+    set_error(ctx, "leaf_depth_histogram: nbins must be 1..64");
+    return TAPAS_B200_ERR_ARG;
+  }
+  cudaStream_t s = ctx->stream;
+  TB_CUDA(ctx, ctx->counters.ensure(64, s));
+  TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 64 * sizeof(unsigned long long), s));
+  const int64_t nl = ctx->n_nonempty_leaves;
+  if (nl > 0) {
+    leaf_depth_hist<<<grid_for(nl, kBlock), kBlock, 0, s>>>(ctx->leaf_list.p, nl, ctx->clevel.p,
+                                                             ctx->cnb.p, nbins, ctx->counters.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  TB_CUDA(ctx, cudaMemcpyAsync(out, ctx->counters.p, nbins * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  return TAPAS_B200_OK;
+}
 
 int ensure_cells(tapas_b200_ctx *ctx, int64_t need, int64_t used) {
   cudaStream_t s = ctx->stream;

@@ -6,4 +6,6 @@ namespace tb {
 int ensure_cells(tapas_b200_ctx *ctx, int64_t need, int64_t used);
 // Builds the tree of the bodies already in ctx->x/y/z/q (ctx->n of them).
 int build_tree(tapas_b200_ctx *ctx, int ncrit);
+// Bodies per leaf depth (deeper leaves in the last bin), nbins <= 64, host out.
+int leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *out);
 }  // namespace tb
