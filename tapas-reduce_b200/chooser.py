@@ -51,6 +51,9 @@ _MIXED_TABLE = [(1e-4, {"P": 8, "theta": 0.4, "ncrit": 64}),
 # features and encodings
 # ---------------------------------------------------------------------------
 def charge_ratio(q) -> float:
+    if not isinstance(q, np.ndarray) and hasattr(q, "abs"):  # device tensor
+        a = float(q.abs().sum())
+        return float(abs(float(q.sum())) / a) if a > 0 else 1.0
     q = np.asarray(q, np.float64)
     a = float(np.sum(np.abs(q)))
     return float(abs(np.sum(q)) / a) if a > 0 else 1.0
@@ -105,7 +108,12 @@ class LearnedChooser:
     def choose(self, features: np.ndarray, tol: float, precisions=(0, 1)) -> dict:
         g = candidate_grid()
         g = g[np.isin(g[:, 3], precisions)]
-        pred = self.predict(encode(features, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
+        # Rank with log10 N inside the training range [4, 6]: the choice only
+        # compares candidates for one system, so relative costs suffice and
+        # the network is not asked to extrapolate in N.
+        f = np.array(features, dtype=np.float64)
+        f[0] = min(max(f[0], 4.0), 6.0)
+        pred = self.predict(encode(f, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
         ok = pred[:, 0] + self.margin <= np.log10(tol)
         if ok.any():
             idx = np.flatnonzero(ok)[np.argmin(pred[ok, 1])]

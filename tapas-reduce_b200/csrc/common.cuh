@@ -187,6 +187,7 @@ struct tapas_b200_ctx {
   tb::TcState tc;                       // mixed: tensor-core M2L work state
   const uint8_t *m2l_use = nullptr;     // FP64 M2L: evaluate only pairs with use[e] != 0
   int64_t tc_classes = 0, tc_tiles = 0, tc_segments = 0, n_m2l_tc = 0;
+  size_t tc_op_budget = (size_t)4 << 30;  // bytes of split-TF32 operators kept at once
   bool have_M = false, have_L = false;
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
 

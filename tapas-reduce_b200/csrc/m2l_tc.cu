@@ -115,13 +115,13 @@ __global__ void segment_starts(const int32_t *__restrict__ flag, const int32_t *
 
 // per class: is it a tensor-core class?
 __global__ void class_tc_flags(const int32_t *__restrict__ seg_start, int64_t nseg, int64_t n,
-                               const uint64_t *__restrict__ keys, int32_t *__restrict__ tcflag,
-                               int32_t *__restrict__ ntiles) {
+                               const uint64_t *__restrict__ keys, int64_t min_count,
+                               int32_t *__restrict__ tcflag, int32_t *__restrict__ ntiles) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
        c += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
     const uint64_t k = keys[b];
-    const bool tc = (k != kKeyEmpty) && (k != kKeyRare) && (e - b) >= kTcMin;
+    const bool tc = (k != kKeyEmpty) && (k != kKeyRare) && (e - b) >= min_count;
     tcflag[c] = tc ? 1 : 0;
     ntiles[c] = tc ? (int32_t)((e - b + kNTile - 1) / kNTile) : 0;
   }
@@ -614,7 +614,25 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   segment_starts<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.flag.p, T.scan.p, n,
                                                                     T.seg_start.p);
   TB_LAUNCH_CHECK(ctx);
-  class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p,
+  // Operator memory is bounded: when more classes qualify than the budget
+  // holds, only the most populated ones run on the tensor cores.
+  int64_t min_count = kTcMin;
+  {
+    const size_t op_bytes = 2 * sizeof(float) * (size_t)S::MP * S::KP;
+    const int64_t max_classes = std::max<int64_t>(1, (int64_t)(ctx->tc_op_budget / op_bytes));
+    if (nseg > max_classes) {
+      std::vector<int32_t> st(nseg);
+      TB_CUDA(ctx, cudaMemcpyAsync(st.data(), T.seg_start.p, sizeof(int32_t) * nseg,
+                                   cudaMemcpyDeviceToHost, s));
+      TB_CUDA(ctx, cudaStreamSynchronize(s));
+      std::vector<int64_t> cnt(nseg);
+      for (int64_t c = 0; c < nseg; c++) cnt[c] = (c + 1 < nseg ? st[c + 1] : n) - st[c];
+      std::nth_element(cnt.begin(), cnt.begin() + (max_classes - 1), cnt.end(),
+                       std::greater<int64_t>());
+      min_count = std::max<int64_t>(kTcMin, cnt[max_classes - 1] + 1);
+    }
+  }
+  class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p, min_count,
                                                       T.tcflag.p, T.ntiles.p);
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(scan_exclusive(ctx, T.tcflag.p, T.tcid.p, nseg, T.tcid.p + nseg));

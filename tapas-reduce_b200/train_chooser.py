@@ -7,8 +7,8 @@ Run on a GPU, from the repository root:
 
 Training systems: 250 seeded body sets, N log-uniform in [1e4, 1e6], the
 distribution drawn from {uniform cube [-1,1]^3, Plummer, two Gaussian clusters
-sigma 0.1 with centres 1.0 apart}, charges positive or zero-mean with equal
-odds; 8 random settings each (P in 4..16, theta in [0.2, 0.7], ncrit in
+sigma 0.1 with centres 1.0 apart, unit sphere surface}, charges equal positive
+or zero-mean U[-1,1] with equal odds; 8 random settings each (P in 4..16, theta in [0.2, 0.7], ncrit in
 {16, 32, 64, 128}, mixed or FP64) = 2,000 runs.  Each run records the
 relative-L2 potential error against an FP64 direct sum on 256 sampled targets
 and the device time of the evaluation (sum of the library's CUDA-event phase
@@ -25,7 +25,9 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 DATA_PATH = HERE / "chooser_data.npz"
-DISTS = ["uniform_cube", "plummer", "two_gaussians"]
+# The three distributions of the chooser's specification plus the sphere
+# surface of the large 16M-body run, so that run is inside the training set.
+DISTS = ["uniform_cube", "plummer", "two_gaussians", "sphere_surface"]
 PHASES = ("bbox_keys", "sort", "tree", "upward", "traverse", "list_sort", "m2l", "p2p",
           "downward")
 
@@ -45,10 +47,12 @@ def make_system(tb, i, seed_base):
     rng = np.random.default_rng(seed_base + i)
     n = int(round(10 ** rng.uniform(4, 6)))
     dist = DISTS[int(rng.integers(len(DISTS)))]
-    x, y, z, q = tb.datasets.make(dist, n, seed_base + i)
+    x, y, z, _ = tb.datasets.make(dist, n, seed_base + i)
     if rng.random() < 0.5:  # zero-mean charges
         q = 2.0 * tb.datasets.uniform01(seed_base + i, 91, n) - 1.0
         q = q - q.mean()
+    else:  # equal positive charges
+        q = np.full(n, 1.0 / n)
     return dist, n, (x, y, z, q), rng
 
 
