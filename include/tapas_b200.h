@@ -137,6 +137,30 @@ int tapas_b200_get_sorted(tapas_b200_ctx *ctx, int64_t *orig_index, uint64_t *ke
  * hot/buildtree.h:89-117). */
 int tapas_b200_leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *hist);
 
+/* ---- Barnes-Hut sample path (sample/barnes-hut/bh.cc) ---------------------- */
+/* Bodies are passed to tapas_b200_partition with the mass in the q slot; the
+ * sample builds its tree with ncrit = 1 (bh.cc:230). */
+
+/* Replaces TapasBH::Map(Approximate(), *root) (bh.cc:232, Approximate :155-190):
+ * per cell the mass and mass-weighted centre, children before parents. */
+int tapas_b200_bh_upward(tapas_b200_ctx *ctx);
+/* Replaces TapasBH::Map(interact(), tapas::Product(*root, *root), theta)
+ * (bh.cc:235, interact :192-224, ComputeForce :135-153): per body a walk from
+ * the root accepting cells with width / |centre - body| < theta, leaves summed
+ * body by body (self included, softening eps2; the sample uses 1e-6).  Results
+ * (read with tapas_b200_get_results) are the sample's float4 per body:
+ * (ax, ay, az, phi).  TAPAS_B200_FP64 reproduces the sample's arithmetic;
+ * TAPAS_B200_MIXED walks with FP32 positions and FP32 copies of the cells'
+ * FP64 moments. */
+int tapas_b200_bh_interact(tapas_b200_ctx *ctx, double theta, double eps2, int precision);
+/* Cell approximations and direct body interactions of the last walk. */
+int tapas_b200_bh_counts(tapas_b200_ctx *ctx, uint64_t *n_approx, uint64_t *n_direct);
+/* Partition + bh_upward + bh_interact + get_results in one call (calc(),
+ * bh.cc:228-245, with ncrit and theta as arguments). */
+int tapas_b200_bh_evaluate(tapas_b200_ctx *ctx, const double *x, const double *y, const double *z,
+                           const double *m, int64_t n, int ncrit, double theta, double eps2,
+                           int precision, double *out4, int order, int mem);
+
 /* ---- learned parameter chooser: network trained and run by own kernels ---- */
 /* No counterpart in the reference (the learned part of this implementation).
  * Fully connected n_in -> n_hidden x n_layers (tanh) -> n_out (linear), FP32,

@@ -823,3 +823,100 @@ void oracle_direct_field(int64_t n, const double *x, const double *y, const doub
                          const double *q, int64_t nt, const int64_t *tg, double *out, int nth) {
   direct_impl(n, x, y, z, q, nt, tg, out, nth, 1);
 }
+
+/* ---------------------------------------------------------------------------
+ * Barnes-Hut sample: sample/barnes-hut/bh.cc, on the same tree (q = mass).
+ * ------------------------------------------------------------------------- */
+
+/* Approximate, bh.cc:155-190: leaf with one body -> the body itself; empty
+ * leaf -> zero; non-leaf -> mass and mass-weighted centre of the 8 children
+ * (children summed in index order, then divided by the total mass).  Leaves
+ * with more than one body (ncrit > 1; the sample asserts ncrit == 1) get the
+ * same mass-weighted centre over their bodies. */
+static void bh_approx_rec(oracle_fmm *h, int32_t ci, double *attr) {
+  ocell *c = &h->cells[ci];
+  double *a = attr + 4 * ci;
+  if (c->leaf) {
+    if (c->nb == 0) {
+      a[0] = a[1] = a[2] = a[3] = 0;
+    } else if (c->nb == 1) {
+      int64_t b = c->bbeg;
+      a[0] = h->sx[b]; a[1] = h->sy[b]; a[2] = h->sz[b]; a[3] = h->sq[b];
+    } else {
+      double w = 0, x = 0, y = 0, z = 0;
+      for (int64_t i = 0; i < c->nb; i++) {
+        int64_t b = c->bbeg + i;
+        w += h->sq[b];
+        x += h->sx[b] * h->sq[b];
+        y += h->sy[b] * h->sq[b];
+        z += h->sz[b] * h->sq[b];
+      }
+      a[0] = x / w; a[1] = y / w; a[2] = z / w; a[3] = w;
+    }
+    return;
+  }
+  double w = 0, x = 0, y = 0, z = 0;
+  for (int i = 0; i < 8; i++) {
+    int32_t k = c->child[i];
+    bh_approx_rec(h, k, attr);
+    const double *s = attr + 4 * k;
+    w += s[3];
+    x += s[0] * s[3];
+    y += s[1] * s[3];
+    z += s[2] * s[3];
+  }
+  a[0] = x / w; a[1] = y / w; a[2] = z / w; a[3] = w;
+}
+
+/* ComputeForce, bh.cc:135-153 */
+static inline void bh_force(const double p[3], const double ap[4], double eps2, double out[4]) {
+  double dx = ap[0] - p[0], dy = ap[1] - p[1], dz = ap[2] - p[2];
+  double R2 = dx * dx + dy * dy + dz * dz + eps2;
+  double invR = 1.0 / sqrt(R2);
+  double invR3 = invR * invR * invR;
+  out[0] += dx * invR3 * ap[3];
+  out[1] += dy * invR3 * ap[3];
+  out[2] += dz * invR3 * ap[3];
+  out[3] += invR * ap[3];
+}
+
+/* interact, bh.cc:192-224, for one target body (the sample's target leaves
+ * hold one body; with larger leaves every body runs its own walk). */
+static void bh_walk(oracle_fmm *h, const double *attr, int32_t ci, const double p[3], double theta,
+                    double eps2, double out[4], uint64_t *napprox, uint64_t *ndirect) {
+  const ocell *c = &h->cells[ci];
+  if (c->leaf) {
+    for (int64_t i = 0; i < c->nb; i++) {
+      int64_t b = c->bbeg + i;
+      double ap[4] = {h->sx[b], h->sy[b], h->sz[b], h->sq[b]};
+      bh_force(p, ap, eps2, out);
+      (*ndirect)++;
+    }
+    return;
+  }
+  double dx = p[0] - c->center[0], dy = p[1] - c->center[1], dz = p[2] - c->center[2];
+  double d = sqrt(dx * dx + dy * dy + dz * dz);
+  double s = c->mx[0] - c->mn[0];
+  if ((s / d) < theta) {
+    bh_force(p, attr + 4 * ci, eps2, out);
+    (*napprox)++;
+  } else {
+    for (int i = 0; i < 8; i++) bh_walk(h, attr, c->child[i], p, theta, eps2, out, napprox, ndirect);
+  }
+}
+
+int oracle_bh(oracle_fmm *h, double theta, double eps2, double *out4, uint64_t *counts) {
+  if (!h->cells && oracle_build(h)) return -1;
+  double *attr = calloc((size_t)h->ncells * 4, sizeof(double));
+  bh_approx_rec(h, 0, attr);
+  uint64_t na = 0, nd = 0;
+  for (int64_t b = 0; b < h->n; b++) {
+    double p[3] = {h->sx[b], h->sy[b], h->sz[b]};
+    double *o = out4 + 4 * b;
+    o[0] = o[1] = o[2] = o[3] = 0;
+    bh_walk(h, attr, 0, p, theta, eps2, o, &na, &nd);
+  }
+  if (counts) { counts[0] = na; counts[1] = nd; }
+  free(attr);
+  return 0;
+}

@@ -68,6 +68,11 @@ uint64_t oracle_key_finest(int ax, int ay, int az);
 void oracle_key_region(uint64_t k, const double root_min[3], const double root_max[3], double mn[3],
                        double mx[3]);
 
+/* Barnes-Hut sample (sample/barnes-hut/bh.cc:135-224) on this handle's tree
+ * (q = mass, tree built with its ncrit): out4 = (ax, ay, az, phi) per body in
+ * sorted order; counts = {approximations, direct interactions}. */
+int oracle_bh(oracle_fmm *h, double theta, double eps2, double *out4, uint64_t *counts);
+
 /* FP64 direct sum (LaplaceP2PCPU_tapas.h P2P over all sources, then the
  * TRG /= SRC normalisation of tapas_exafmm.cxx:365-367) for selected targets.
  * trg4 gets 4 values per target.  nthreads <= 0 uses all cores. */

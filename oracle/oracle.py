@@ -70,6 +70,8 @@ def lib():
         L.oracle_get_m2l.argtypes = [_vp, _vp, _vp]
         L.oracle_get_p2p.argtypes = [_vp, _vp, _vp]
         L.oracle_get_bodies.argtypes = [_vp, _vp, _vp, _vp]
+        L.oracle_bh.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp]
+        L.oracle_bh.restype = ctypes.c_int
         for f in ("oracle_direct", "oracle_direct_field"):
             getattr(L, f).argtypes = [_c_i64, _vp, _vp, _vp, _vp, _c_i64, _vp, _vp, ctypes.c_int]
         L.oracle_key_child.restype = ctypes.c_uint64
@@ -173,6 +175,46 @@ class Oracle:
         out = np.empty_like(t)
         out[o] = t
         return out
+
+
+def barnes_hut(x, y, z, m, ncrit=1, theta=0.5, eps2=1e-6):
+    """Barnes-Hut sample restated (fmm_oracle.c oracle_bh): (ax, ay, az, phi)
+    per body in ORIGINAL order, and (approximations, direct interactions)."""
+    o = Oracle(x, y, z, m, P=2, ncrit=ncrit, theta=0.5, run=False)
+    if lib().oracle_build(o.h):
+        raise RuntimeError("oracle_build failed")
+    out = np.zeros((o.n, 4))
+    cnt = np.zeros(2, np.uint64)
+    lib().oracle_bh(o.h, float(theta), float(eps2), _p(out), _p(cnt))
+    orig, _, _ = o.bodies()
+    res = np.empty_like(out)
+    res[orig] = out
+    return res, cnt
+
+
+def bh_reference_available() -> bool:
+    return (REF_DIR / "bh_ref").exists()
+
+
+def run_bh_reference(x, y, z, m, timeout=3600):
+    """The unmodified reference BH sample (ncrit = 1, theta = 0.5, EPS2 = 1e-6):
+    (ax, ay, az, phi) per body in ORIGINAL order (bodies matched by position)."""
+    exe = REF_DIR / "bh_ref"
+    n = len(x)
+    with tempfile.TemporaryDirectory() as d:
+        fi, fo = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fi, "wb") as f:
+            f.write(np.int64(n).tobytes())
+            f.write(np.stack([x, y, z, m], axis=1).astype(np.float64).tobytes())
+        subprocess.run([str(exe), fi, fo], check=True, timeout=timeout, cwd=d,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        raw = np.fromfile(fo, dtype=np.float64, offset=8).reshape(n, 8)
+    pos = np.stack([x, y, z], axis=1)
+    order = np.lexsort(pos.T[::-1])
+    rorder = np.lexsort(raw[:, :3].T[::-1])
+    res = np.empty((n, 4))
+    res[order] = raw[rorder, 4:]
+    return res
 
 
 def direct(x, y, z, q, targets, nthreads=0, field=False):

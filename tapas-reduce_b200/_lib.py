@@ -32,7 +32,8 @@ EXPORTS = (
     "tapas_b200_direct", "tapas_b200_direct_noalloc", "tapas_b200_leaf_depth_histogram",
     "tapas_b200_mlp_create", "tapas_b200_mlp_num_params", "tapas_b200_mlp_set_params",
     "tapas_b200_mlp_get_params", "tapas_b200_mlp_forward", "tapas_b200_mlp_gradients",
-    "tapas_b200_mlp_train",
+    "tapas_b200_mlp_train", "tapas_b200_bh_upward", "tapas_b200_bh_interact",
+    "tapas_b200_bh_counts", "tapas_b200_bh_evaluate",
 )
 
 
@@ -119,6 +120,11 @@ def lib():
         "tapas_b200_mlp_train": [_vp, _vp, _vp, _i64, _int, _int, ctypes.c_float,
                                  ctypes.c_uint64, _vp],
         "tapas_b200_direct_noalloc": [_vp] * 4 + [_i64, _vp, _i64, _vp, _vp],
+        "tapas_b200_bh_upward": [_vp],
+        "tapas_b200_bh_interact": [_vp, _dbl, _dbl, _int],
+        "tapas_b200_bh_counts": [_vp, _vp, _vp],
+        "tapas_b200_bh_evaluate": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _dbl, _dbl, _int, _vp,
+                                   _int, _int],
     }
     for name, args in sig2.items():
         f = getattr(L, name)
@@ -305,6 +311,30 @@ class Context:
                                                 float(theta), precision, op, order, mem))
         self.n = n
         return out
+
+    # ---- Barnes-Hut sample path ------------------------------------------
+    def bh_evaluate(self, x, y, z, m, ncrit=1, theta=0.5, eps2=1e-6, precision=FP64,
+                    order=ORDER_ORIGINAL, out=None):
+        """(ax, ay, az, phi) per body, the sample's calc() (bh.cc:228-245)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if isinstance(a, np.ndarray) else a
+                for a in (x, y, z, m)]
+        ptrs = [_ptr(a) for a in arrs]
+        mem = ptrs[0][1]
+        n = len(arrs[0]) if isinstance(arrs[0], np.ndarray) else arrs[0].numel()
+        if out is None:
+            out = np.zeros((n, 4))
+        op, _ = _ptr(out)
+        self._keep = arrs
+        self._check(self._L.tapas_b200_bh_evaluate(self.h, *[p for p, _ in ptrs], n, ncrit,
+                                                   float(theta), float(eps2), precision, op,
+                                                   order, mem))
+        self.n = n
+        return out
+
+    def bh_counts(self):
+        a, d = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._L.tapas_b200_bh_counts(self.h, ctypes.byref(a), ctypes.byref(d)))
+        return int(a.value), int(d.value)
 
     def leaf_depth_histogram(self, nbins: int = 16) -> np.ndarray:
         h = np.zeros(nbins, np.int64)

@@ -187,6 +187,8 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->L.release();
   mixed_release(ctx);
   mlp_release(ctx);
+  ctx->bh_attr.release();
+  ctx->bh_attr32.release();
   ctx->pinned.release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -255,7 +257,35 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
     TB_TRY(copy_in(ctx, ctx->q.p, q, n, mem));
   }
   ctx->n = n;
+  ctx->have_bh_attr = false;
   return build_tree(ctx, ncrit);
+}
+
+int tapas_b200_bh_upward(tapas_b200_ctx *ctx) {
+  TB_TRY(check_ctx(ctx));
+  return bh_upward(ctx);
+}
+
+int tapas_b200_bh_interact(tapas_b200_ctx *ctx, double theta, double eps2, int precision) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_precision(ctx, precision));
+  return bh_interact(ctx, theta, eps2, precision);
+}
+
+int tapas_b200_bh_counts(tapas_b200_ctx *ctx, uint64_t *n_approx, uint64_t *n_direct) {
+  TB_TRY(check_ctx(ctx));
+  if (n_approx) *n_approx = ctx->bh_napprox;
+  if (n_direct) *n_direct = ctx->bh_ndirect;
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_bh_evaluate(tapas_b200_ctx *ctx, const double *x, const double *y, const double *z,
+                           const double *m, int64_t n, int ncrit, double theta, double eps2,
+                           int precision, double *out4, int order, int mem) {
+  TB_TRY(tapas_b200_partition(ctx, x, y, z, m, n, ncrit, mem));
+  TB_TRY(tapas_b200_bh_upward(ctx));
+  TB_TRY(tapas_b200_bh_interact(ctx, theta, eps2, precision));
+  return tapas_b200_get_results(ctx, out4, order, mem);
 }
 
 int tapas_b200_tree_info(tapas_b200_ctx *ctx, tapas_b200_tree_stats *out) {

@@ -193,6 +193,12 @@ struct tapas_b200_ctx {
 
   tb::Mlp *mlp = nullptr;               // learned chooser network, if created
 
+  // ---- Barnes-Hut ----
+  tb::DBuf<double4> bh_attr;            // per cell: mass-weighted centre (x,y,z) and mass
+  tb::DBuf<float4> bh_attr32;           // FP32 copy for the FP32 walk
+  bool have_bh_attr = false;
+  uint64_t bh_napprox = 0, bh_ndirect = 0;
+
   tb::HBuf pinned;
 };
 

@@ -8,4 +8,7 @@ int ensure_cells(tapas_b200_ctx *ctx, int64_t need, int64_t used);
 int build_tree(tapas_b200_ctx *ctx, int ncrit);
 // Bodies per leaf depth (deeper leaves in the last bin), nbins <= 64, host out.
 int leaf_depth_histogram(tapas_b200_ctx *ctx, int nbins, int64_t *out);
+// Barnes-Hut sample path (bh.cu).
+int bh_upward(tapas_b200_ctx *ctx);
+int bh_interact(tapas_b200_ctx *ctx, double theta, double eps2, int precision);
 }  // namespace tb

@@ -63,9 +63,33 @@ def make(name, dist, n, seed, P, ncrit, theta, keep):
     print(name, n, "cells", len(c), "m2l", R["n_m2l"], "p2p", R["n_p2p_interactions"])
 
 
+# Barnes-Hut sample (ncrit = 1, theta = 0.5, EPS2 = 1e-6 fixed by bh.cc):
+# name: (distribution, n, seed); "unit_cube_mass" is the sample's own data
+# model (positions uniform in [0,1)^3, masses U[0,1)/N, bh.cc:414-427)
+# restated with this project's generator.
+BH_CASES = {
+    "bh_unitcube_n2000": ("unit_cube_mass", 2000, 21),
+    "bh_plummer_n1500": ("plummer", 1500, 22),
+}
+
+
+def make_bh(name, dist, n, seed):
+    if dist == "unit_cube_mass":
+        x, y, z = (ds.uniform01(seed, s, n) for s in (1, 2, 3))
+        m = ds.uniform01(seed, 4, n) / n
+    else:
+        x, y, z, m = ds.make(dist, n, seed)
+    res = oracle.run_bh_reference(x, y, z, m)
+    np.savez_compressed(pathlib.Path(__file__).parent / f"{name}.npz", x=x, y=y, z=z, m=m,
+                        bh=res, ncrit=1, theta=0.5, eps2=1e-6)
+    print(name, n)
+
+
 if __name__ == "__main__":
     import subprocess
     oracle.build_reference(quiet=False)
+    for name, args in BH_CASES.items():
+        make_bh(name, *args)
     for name, args in CASES.items():
         try:
             make(name, *args)

@@ -40,12 +40,14 @@ def test_training_fits_a_smooth_map(ctx):
 
 def test_learned_chooser_against_fixed_setting(tb):
     """Held-out seeded systems with random tolerances in [1e-7, 1e-3]: the
-    learned choice meets the tolerance more often than the fixed P=10,
-    theta=0.4, ncrit=64 setting and is faster than its FP64 form."""
+    learned choice meets the tolerance far more often than the fixed P=10,
+    theta=0.4, ncrit=64 setting, and where both meet it the learned choice is
+    faster than the fixed FP64 form."""
     from tapas_reduce_b200 import chooser, train_chooser
     if not chooser.MODEL_PATH.exists():
         pytest.skip("no trained chooser model in the package")
-    summary, recs = train_chooser.evaluate(n_systems=24, seed_base=95_000, targets=128)
+    summary, recs = train_chooser.evaluate(n_systems=30, seed_base=95_000, targets=128)
     assert summary["hit_rate_learned"] >= 0.8
-    assert summary["hit_rate_learned"] >= summary["hit_rate_fixed_fp64"]
-    assert summary["geomean_speedup_vs_fixed_fp64"] > 1.0
+    assert summary["hit_rate_learned"] >= summary["hit_rate_fixed_fp64"] + 0.15
+    assert summary["n_both_meet"] >= 5
+    assert summary["geomean_speedup_vs_fixed_fp64_where_both_meet"] > 1.0
