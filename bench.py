@@ -158,6 +158,14 @@ def sum_over_ranks(pg, v: float) -> float:
     return float(t.item())
 
 
+def replica_throughput(pg, ms: float, n: int):
+    """Whole-job throughput of independent replicas: every rank's bodies over
+    the slowest rank's step time.  Returns (max ms, total bodies, bodies/s)."""
+    ms_max = max_over_ranks(pg, ms)
+    n_total = sum_over_ranks(pg, float(n))
+    return ms_max, n_total, n_total / (ms_max * 1e-3)
+
+
 # ---------------------------------------------------------------------------
 # reference CPU implementation (oracle/_ref, built from the reference sources)
 # ---------------------------------------------------------------------------
@@ -182,9 +190,9 @@ def cpu_reference_run(tb, orc, n=REF_SAMPLE_N, seed=77):
     return n / secs, kind, secs
 
 
-def cpu_baseline_obj(value, kind, secs):
+def cpu_baseline_obj(value, kind, secs, n=REF_SAMPLE_N):
     return {"value": value, "unit": "particles/s", "cores": 1, "kind": kind,
-            "sample": f"{REF_SAMPLE_N} bodies of the same sphere-surface workload, "
+            "sample": f"{n} bodies of the same sphere-surface workload, "
                       f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (meets 1e-6 on it), "
                       f"1 rank x 1 thread (the reference's Serial threading), {secs:.2f} s"}
 
@@ -197,18 +205,19 @@ def run_reference_arm(args):
     orc = load_oracle()
     vals = []
     kind = secs = None
+    ns = args.ref_sample
     for i in range(args.warmup + args.steps):
-        v, kind, secs = cpu_reference_run(tb, orc, seed=77 + i)
+        v, kind, secs = cpu_reference_run(tb, orc, n=ns, seed=77 + i)
         if i >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": REF_SAMPLE_N / value * 1e3, "higher_is_better": True,
+            "ms_per_step": ns / value * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{WORKLOAD} sample n={REF_SAMPLE_N}", "P": REF_P,
+            "config": {"workload": f"{WORKLOAD} sample n={ns}", "P": REF_P,
                        "theta": REF_THETA, "ncrit": REF_NCRIT},
-            "cpu_baseline": cpu_baseline_obj(value, kind, secs),
+            "cpu_baseline": cpu_baseline_obj(value, kind, secs, ns),
             "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "gpu_launches": 0}
@@ -247,6 +256,8 @@ def main():
     ap.add_argument("--targets", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=REF_SAMPLE_N,
+                    help="bodies per reference CPU step (--impl reference)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -319,9 +330,7 @@ def main():
     launches = ctx.kernel_launches() // args.steps
     ctx.set_profiling(False)
     clocks = clk.summary()
-    ms_max = max_over_ranks(pg, ms)
-    n_total = sum_over_ranks(pg, n)
-    value = n_total / (ms_max * 1e-3)
+    ms_max, n_total, value = replica_throughput(pg, ms, n)
     phases = {k: v / args.steps for k, v in phase_acc.items()}
     li = ctx.list_info()
     ti = ctx.tree_info()
