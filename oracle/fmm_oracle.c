@@ -2,8 +2,9 @@
  * CPU restatement of the reference Tapas/ExaFMM N-body evaluation path.
  *
  * TEST INFRASTRUCTURE ONLY (the checker, never the product): see
- * fmm_oracle.h.  Parity pin: tests/test_oracle_vs_reference.py compares this
- * file's output with the unmodified reference built in oracle/_ref, and
+ * fmm_oracle.h.  Parity pin: tests/test_oracle_golden.py compares this file's
+ * output bit for bit with golden vectors that the unmodified reference, built
+ * in oracle/_ref, produced (tests/golden/make_golden.py), and
  * tests/test_oracle_keys.py replays cpp/tests/test_morton_key.cpp.
  *
  * Build for x86-64 without FMA contraction (-ffp-contract=off, no -march):
