@@ -7,9 +7,11 @@
 // grouped by TARGET leaf (CSR) and one warp owns a target leaf at a time:
 //  - warps take target leaves from a global queue ordered by decreasing work
 //    (nt * sum of source bodies), so long interaction lists start first;
-//  - each lane keeps kR targets in registers (kR = ceil(nt/32), a template
-//    parameter, so no issue slot is spent on unused target slots); leaves of
-//    <= 16 bodies are replicated over 32/nt lane groups that split the sources;
+//  - each lane keeps kR targets in registers (kR a template parameter, so no
+//    issue slot is spent on unused target slots); FP64: kR = ceil(nt/32);
+//    mixed: the targets take L = ceil(nt/kR) lanes and the warp holds
+//    G = 32/L copies of them that split the sources, with kR chosen so that
+//    kR/G (time per source) is least;
 //  - source bodies are staged in the warp's shared-memory slice and read as
 //    broadcasts; each target's sum is written once, without atomics.
 //
@@ -20,7 +22,8 @@
 // kept as FP32 (hi, lo) offsets from the body's leaf centre; a source is moved
 // into the target leaf's frame with an error-free sum (TwoSum) of its hi part
 // and the FP64 centre difference, so the separation x_i - x_j is formed from
-// ~47-bit operands and rounds once.  1/r is rsqrtf refined by one Newton step.
+// ~47-bit operands and rounds once.  1/r is rsqrtf (its 2-ulp error is far below
+// the near field's summation error, so no Newton step).
 // Each source leaf is summed in plain FP32 and the partial is Kahan-added into
 // the target's (sum, compensation) pair; the final near field is FP64.
 #include <algorithm>
@@ -33,8 +36,12 @@ namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = 32 * kWarps;
-constexpr int kStage = 64;   // source bodies staged per warp at a time
+constexpr int kStage = 32;   // source bodies staged per warp at a time (one per lane)
 constexpr int kMaxR = 4;     // targets per lane: leaves up to 128 bodies per pass
+// mixed kernel: 4-warp CTAs, 3 per SM (up to 170 registers a thread, 12 warps per SM)
+constexpr int kMixedWarps = 4;
+constexpr int kMixedThreads = 32 * kMixedWarps;
+constexpr int kMixedBlocks = 3;
 
 // ---------------------------------------------------------------------------
 // work order: target leaves by decreasing nt * sum(ns)
@@ -190,63 +197,144 @@ __device__ __forceinline__ float two_sum(float a, float b, float &e) {
   return s;
 }
 
+// Shape of a mixed tile of nt targets: kR targets per lane, L = ceil(nt/kR)
+// lanes per group, G = 32/L groups that split the sources.  Time per source
+// ~ kR / G, so pick the kR in 1..kMaxR that minimises it (ties: the larger
+// kR, fewer shared loads per interaction).  nt <= 32 * kMaxR.
+__device__ __forceinline__ void mixed_shape(int nt, int &R, int &L, int &G) {
+  R = kMaxR;
+  L = (nt + kMaxR - 1) / kMaxR;
+  G = 32 / L;
+#pragma unroll
+  for (int r = kMaxR - 1; r >= 1; r--) {
+    const int l = (nt + r - 1) / r;
+    if (l > 32) break;
+    const int g = 32 / l;
+    if (r * G < R * g) {
+      R = r;
+      L = l;
+      G = g;
+    }
+  }
+}
+
+// A staged source body in the target leaf's frame: FP32 hi part and charge,
+// FP32 lo part.
+struct __align__(16) SrcRec {
+  float4 hi, lo;
+};
+
+// A source leaf of the current batch: body range and centre offset from the
+// target leaf (FP64 difference as FP32 hi + lo).
+struct __align__(16) LeafMeta {
+  int b0, ns;
+  float hx, hy, hz, lx, ly, lz;
+};
+
+// One tile of a target leaf: lane (g, l) = (lane / L, lane % L) holds targets
+// l, l + L, ..., l + (kR-1) L and takes every G-th staged source.
+//
+// The source leaves of the target's list are read 32 at a time: lane j loads
+// list entry j's leaf range and its centre offset (the FP64 difference split
+// into FP32 hi + lo) into the warp's table in shared memory, so the dependent
+// list -> cell loads are paid once per 32 source leaves.  Source bodies move
+// through the warp's shared-memory slice 32 at a time; the next chunk's
+// global loads are issued before the current chunk is computed.
 template <int kR>
 __device__ __forceinline__ void mixed_tile(
-    int lane, int wi, int tb0, int nt, int G, int g, int e0, int e1, double tcx, double tcy,
+    int lane, int wi, int tb0, int nt, int L, int G, int e0, int e1, double tcx, double tcy,
     double tcz, const uint64_t *__restrict__ list, uint64_t mask, const int32_t *__restrict__ cbeg,
     const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
-    const float4 *__restrict__ rel_hi, const float4 *__restrict__ rel_lo, float4 (*shi)[kStage],
-    float4 (*slo)[kStage], double4 (*red)[32], double *__restrict__ trg) {
+    const float4 *__restrict__ rel_hi, const float4 *__restrict__ rel_lo, SrcRec (*ss)[kStage],
+    LeafMeta (*mt)[32], double4 (*red)[32], double *__restrict__ trg) {
+  const int g = lane / L, tl = lane - g * L;
   const bool active = g < G;
-  const int tl = (G > 1) ? lane % nt : lane;
+  const int gs = active ? g : kStage;  // idle lanes skip the source loop
   float txh[kR], tyh[kR], tzh[kR], txl[kR], tyl[kR], tzl[kR];
   float ps[kR], pc[kR], xs[kR], xc[kR], ys[kR], yc[kR], zs[kR], zc[kR];
+  float tp[kR], tx[kR], ty[kR], tz[kR];
 #pragma unroll
   for (int r = 0; r < kR; r++) {
-    const int t = tl + 32 * r;
+    const int t = tl + L * r;
     const bool v = active && t < nt;
     const float4 h = v ? rel_hi[tb0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 l = v ? rel_lo[tb0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
     txh[r] = h.x; tyh[r] = h.y; tzh[r] = h.z;
     txl[r] = l.x; tyl[r] = l.y; tzl[r] = l.z;
     ps[r] = pc[r] = xs[r] = xc[r] = ys[r] = yc[r] = zs[r] = zc[r] = 0.f;
+    tp[r] = tx[r] = ty[r] = tz[r] = 0.f;
   }
-  for (int e = e0; e < e1; e++) {
-    const int s = (int)(list[e] & mask);
-    const int sb0 = cbeg[s], ns = cnb[s];
-    // source frame -> target frame: FP64 centre difference as (hi, lo) floats
-    const double dcx = ccen[3 * s] - tcx, dcy = ccen[3 * s + 1] - tcy,
-                 dcz = ccen[3 * s + 2] - tcz;
-    const float shx = (float)dcx, shy = (float)dcy, shz = (float)dcz;
-    const float slx = (float)(dcx - shx), sly = (float)(dcy - shy), slz = (float)(dcz - shz);
-    for (int chunk = 0; chunk < ns; chunk += kStage) {
-      const int cnt = min(kStage, ns - chunk);
+  LeafMeta *const meta = mt[wi];
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int nbat = min(32, e1 - eb);
+    __syncwarp();
+    if (lane < nbat) {
+      const int s = (int)(list[eb + lane] & mask);
+      LeafMeta m;
+      m.b0 = cbeg[s];
+      m.ns = cnb[s];
+      // source frame -> target frame: FP64 centre difference as (hi, lo) floats
+      const double dcx = ccen[3 * s] - tcx, dcy = ccen[3 * s + 1] - tcy,
+                   dcz = ccen[3 * s + 2] - tcz;
+      m.hx = (float)dcx; m.hy = (float)dcy; m.hz = (float)dcz;
+      m.lx = (float)(dcx - m.hx); m.ly = (float)(dcy - m.hy); m.lz = (float)(dcz - m.hz);
+      meta[lane] = m;
+    }
+    __syncwarp();
+    // first non-empty source leaf of the batch
+    int j = 0;
+    int ns_j = meta[0].ns;
+    while (ns_j == 0 && ++j < nbat) ns_j = meta[j].ns;
+    if (j >= nbat) continue;
+    int ch = 0;
+    float4 ph = make_float4(0.f, 0.f, 0.f, 0.f), pl = ph;
+    {
+      const int b0 = meta[j].b0;
+      if (lane < min(kStage, ns_j)) {
+        ph = rel_hi[b0 + lane];
+        pl = rel_lo[b0 + lane];
+      }
+    }
+    while (j < nbat) {
+      const int cnt = min(kStage, ns_j - ch);
       __syncwarp();
-      for (int k = lane; k < cnt; k += 32) {
-        const float4 h = rel_hi[sb0 + chunk + k];
-        const float4 l = rel_lo[sb0 + chunk + k];
+      if (lane < cnt) {
+        const LeafMeta &m = meta[j];
         float ex, ey, ez;
-        const float ax = two_sum(h.x, shx, ex), ay = two_sum(h.y, shy, ey),
-                    az = two_sum(h.z, shz, ez);
-        shi[wi][k] = make_float4(ax, ay, az, h.w);
-        slo[wi][k] = make_float4(ex + (l.x + slx), ey + (l.y + sly), ez + (l.z + slz), 0.f);
+        const float ax = two_sum(ph.x, m.hx, ex), ay = two_sum(ph.y, m.hy, ey),
+                    az = two_sum(ph.z, m.hz, ez);
+        ss[wi][lane].hi = make_float4(ax, ay, az, ph.w);
+        ss[wi][lane].lo =
+            make_float4(ex + (pl.x + m.lx), ey + (pl.y + m.ly), ez + (pl.z + m.lz), 0.f);
       }
       __syncwarp();
-      float tp[kR], tx[kR], ty[kR], tz[kR];
-#pragma unroll
-      for (int r = 0; r < kR; r++) tp[r] = tx[r] = ty[r] = tz[r] = 0.f;
-      for (int k = g; k < cnt; k += G) {
-        const float4 bh = shi[wi][k];
-        const float4 bl = slo[wi][k];
+      // next chunk: the rest of this leaf, else the next non-empty leaf of the batch
+      int j2 = j, ch2 = ch + kStage, ns2 = ns_j;
+      const bool leaf_done = ch2 >= ns_j;
+      if (leaf_done) {
+        ch2 = 0;
+        ns2 = 0;
+        while (ns2 == 0 && ++j2 < nbat) ns2 = meta[j2].ns;
+      }
+      if (j2 < nbat) {
+        const int b0 = meta[j2].b0;
+        if (lane < min(kStage, ns2 - ch2)) {
+          ph = rel_hi[b0 + ch2 + lane];
+          pl = rel_lo[b0 + ch2 + lane];
+        }
+      }
+      // two sources in flight: their rsqrt latencies overlap
+#pragma unroll 2
+      for (int k = gs; k < cnt; k += G) {
+        const float4 bh = ss[wi][k].hi;
+        const float4 bl = ss[wi][k].lo;
 #pragma unroll
         for (int r = 0; r < kR; r++) {
           const float dx = (txh[r] - bh.x) + (txl[r] - bl.x);
           const float dy = (tyh[r] - bh.y) + (tyl[r] - bl.y);
           const float dz = (tzh[r] - bh.z) + (tzl[r] - bl.z);
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float ri = rsqrtf(r2);
-          ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);  // one Newton step
-          ri = r2 > 0.f ? ri : 0.f;
+          const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
           const float qr = bh.w * ri;
           const float qr3 = qr * ri * ri;
           tp[r] += qr;
@@ -255,13 +343,20 @@ __device__ __forceinline__ void mixed_tile(
           tz[r] = fmaf(dz, qr3, tz[r]);
         }
       }
+      if (leaf_done) {
+        // one source leaf summed in FP32: Kahan-add it into the target's sums
 #pragma unroll
-      for (int r = 0; r < kR; r++) {
-        kahan_add(ps[r], pc[r], tp[r]);
-        kahan_add(xs[r], xc[r], tx[r]);
-        kahan_add(ys[r], yc[r], ty[r]);
-        kahan_add(zs[r], zc[r], tz[r]);
+        for (int r = 0; r < kR; r++) {
+          kahan_add(ps[r], pc[r], tp[r]);
+          kahan_add(xs[r], xc[r], tx[r]);
+          kahan_add(ys[r], yc[r], ty[r]);
+          kahan_add(zs[r], zc[r], tz[r]);
+          tp[r] = tx[r] = ty[r] = tz[r] = 0.f;
+        }
       }
+      j = j2;
+      ch = ch2;
+      ns_j = ns2;
     }
   }
 #pragma unroll
@@ -274,25 +369,25 @@ __device__ __forceinline__ void mixed_tile(
       __syncwarp();
       if (g == 0) {
         for (int gg = 1; gg < G; gg++) {
-          const double4 o = red[wi][lane + gg * nt];
+          const double4 o = red[wi][tl + gg * L];
           v.x += o.x; v.y += o.y; v.z += o.z; v.w += o.w;
         }
       }
     }
-    const int t = tl + 32 * r;
+    const int t = tl + L * r;
     if (active && g == 0 && t < nt) reinterpret_cast<double4 *>(trg)[tb0 + t] = v;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) p2p_mixed_kernel(
+__global__ void __launch_bounds__(kMixedThreads, kMixedBlocks) p2p_mixed_kernel(
     const uint32_t *__restrict__ order, int64_t nleaves, int *__restrict__ counter,
     const int32_t *__restrict__ off, const uint64_t *__restrict__ list, uint64_t src_mask,
     const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
     const double *__restrict__ ccen, const float4 *__restrict__ rel_hi,
     const float4 *__restrict__ rel_lo, double *__restrict__ trg) {
-  __shared__ float4 shi[kWarps][kStage];
-  __shared__ float4 slo[kWarps][kStage];
-  __shared__ double4 red[kWarps][32];
+  __shared__ SrcRec ss[kMixedWarps][kStage];
+  __shared__ LeafMeta mt[kMixedWarps][32];
+  __shared__ double4 red[kMixedWarps][32];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   for (;;) {
     const int w = next_leaf(counter, lane);
@@ -303,12 +398,11 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed_kernel(
     const double tcx = ccen[3 * c], tcy = ccen[3 * c + 1], tcz = ccen[3 * c + 2];
     for (int tbase = 0; tbase < nt_all; tbase += 32 * kMaxR) {
       const int nt = min(nt_all - tbase, 32 * kMaxR);
-      const int G = nt <= 16 ? 32 / nt : 1;
-      const int g = nt <= 16 ? lane / nt : 0;
-      const int R = (nt + 31) / 32;
+      int R, L, G;
+      mixed_shape(nt, R, L, G);
 #define TB_MIXED_TILE(RR)                                                                     \
-  mixed_tile<RR>(lane, wi, tb0 + tbase, nt, G, g, e0, e1, tcx, tcy, tcz, list, src_mask, cbeg, \
-                 cnb, ccen, rel_hi, rel_lo, shi, slo, red, trg)
+  mixed_tile<RR>(lane, wi, tb0 + tbase, nt, L, G, e0, e1, tcx, tcy, tcz, list, src_mask, cbeg, \
+                 cnb, ccen, rel_hi, rel_lo, ss, mt, red, trg)
       if (R == 1) TB_MIXED_TILE(1);
       else if (R == 2) TB_MIXED_TILE(2);
       else if (R == 3) TB_MIXED_TILE(3);
@@ -347,11 +441,11 @@ int p2p_order(tapas_b200_ctx *ctx) {
   return TAPAS_B200_OK;
 }
 
-int p2p_grid(tapas_b200_ctx *ctx) {
+int p2p_grid(tapas_b200_ctx *ctx, int warps_per_block) {
   // persistent: enough warps to fill the GPU, never more than the leaves
   const int64_t nl = ctx->n_nonempty_leaves;
-  int64_t g = (int64_t)ctx->num_sms * 8;
-  const int64_t need = (nl + kWarps - 1) / kWarps;
+  int64_t g = (int64_t)ctx->num_sms * (64 / warps_per_block);
+  const int64_t need = (nl + warps_per_block - 1) / warps_per_block;
   return (int)std::max<int64_t>(1, std::min(g, need));
 }
 
@@ -363,7 +457,7 @@ int p2p_fp64(tapas_b200_ctx *ctx) {
   if (nl == 0) return TAPAS_B200_OK;
   TB_TRY(p2p_order(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
-  p2p_fp64_kernel<<<p2p_grid(ctx), kThreads, 0, s>>>(
+  p2p_fp64_kernel<<<p2p_grid(ctx, kWarps), kThreads, 0, s>>>(
       ctx->p2p_order.p, nl, ctx->p2p_counter.p, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cbeg.p,
       ctx->cnb.p, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->trg.p);
   TB_LAUNCH_CHECK(ctx);
@@ -383,7 +477,7 @@ int p2p_mixed(tapas_b200_ctx *ctx) {
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(p2p_order(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
-  p2p_mixed_kernel<<<p2p_grid(ctx), kThreads, 0, s>>>(
+  p2p_mixed_kernel<<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
       ctx->p2p_order.p, nl, ctx->p2p_counter.p, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cbeg.p,
       ctx->cnb.p, ctx->ccen.p, ctx->rel4.p, ctx->rel_lo.p, ctx->trg.p);
   TB_LAUNCH_CHECK(ctx);
