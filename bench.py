@@ -283,6 +283,10 @@ def main():
     ap.add_argument("--n", type=int, default=16_000_000)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--targets", type=int, default=4000)
+    ap.add_argument("--P", type=int, default=0, help="with --theta and --ncrit: fixed setting "
+                                                     "instead of the learned choice")
+    ap.add_argument("--theta", type=float, default=0.0)
+    ap.add_argument("--ncrit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=REF_SAMPLE_N,
@@ -315,8 +319,14 @@ def main():
     # table's setting is used instead.
     from importlib import import_module
     chooser = import_module("tapas_reduce_b200.chooser")
-    feats = chooser.system_features(ctx, *dev)
-    prm = chooser.choose_params(n, args.tol, "mixed", features=feats, ctx=ctx)
+    if args.P and args.theta and args.ncrit:
+        # fixed setting (profiling a given configuration); still verified
+        prm = {"P": args.P, "theta": args.theta, "ncrit": args.ncrit, "precision": "mixed",
+               "source": "fixed by --P/--theta/--ncrit"}
+        ctx.partition(*dev, ncrit=args.ncrit)  # the direct-sum check reads the bodies
+    else:
+        feats = chooser.system_features(ctx, *dev)
+        prm = chooser.choose_params(n, args.tol, "mixed", features=feats, ctx=ctx)
     d_check = ctx.direct(tg)
     try:
         ctx.evaluate(*dev, P=prm["P"], ncrit=prm["ncrit"], theta=prm["theta"],

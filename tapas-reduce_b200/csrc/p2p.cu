@@ -22,11 +22,12 @@
 // kept as FP32 (hi, lo) offsets from the body's leaf centre; a source is moved
 // into the target leaf's frame with an error-free sum (TwoSum) of its hi part
 // and the FP64 centre difference, so the separation x_i - x_j is formed from
-// ~47-bit operands and rounds once.  1/r is rsqrtf (its 2-ulp error is far below
+// ~47-bit operands and rounds once.  1/r is the hardware rsqrt (its error is far below
 // the near field's summation error, so no Newton step).
 // Each source leaf is summed in plain FP32 and the partial is Kahan-added into
 // the target's (sum, compensation) pair; the final near field is FP64.
 #include <algorithm>
+#include <cfloat>
 
 #include "kernels.cuh"
 #include "primitives.cuh"
@@ -218,6 +219,15 @@ __device__ __forceinline__ void mixed_shape(int nt, int &R, int &L, int &G) {
   }
 }
 
+// 1/sqrt(x) for normal x > 0 from the hardware approximation (relative error
+// below 2^-22.9), without the denormal rescaling rsqrtf adds; callers treat
+// x < FLT_MIN (a separation below ~1e-19) as coincident bodies.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // A staged source body in the target leaf's frame: FP32 hi part and charge,
 // FP32 lo part.
 struct __align__(16) SrcRec {
@@ -334,7 +344,7 @@ __device__ __forceinline__ void mixed_tile(
           const float dy = (tyh[r] - bh.y) + (tyl[r] - bl.y);
           const float dz = (tzh[r] - bh.z) + (tzl[r] - bl.z);
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+          const float ri = r2 >= FLT_MIN ? rsqrt_ftz(r2) : 0.f;
           const float qr = bh.w * ri;
           const float qr3 = qr * ri * ri;
           tp[r] += qr;
