@@ -20,7 +20,8 @@
 //     unit-width singular harmonics and split into TF32 hi + lo parts, laid
 //     out as K-major core matrices (8 rows x 16 bytes) ready for smem.
 //  4. GEMM kernel: a CTA takes tiles of 128 pairs of one class; K is streamed
-//     in chunks through a 2-stage shared-memory ring; one thread issues
+//     in chunks through a 2-4 stage shared-memory ring filled by cp.async
+//     (operator chunks and the pre-split multipole rows); one thread issues
 //     tcgen05.mma kind::tf32 (M=128 rows of T per M-tile, N=128 pairs, K=8)
 //     three times per k-step (hi*hi + lo*hi + hi*lo: split-precision
 //     "3xTF32", FP32 accumulation in TMEM); completion via tcgen05.commit to
@@ -57,7 +58,13 @@ struct TcShape {
   static constexpr int TMEM_COLS = MT == 1 ? 128 : (MT == 2 ? 256 : 512);
   // one stage: A hi/lo (MP x KC) + B hi/lo (128 x KC) floats
   static constexpr int STAGE_FLOATS = 2 * MP * KC + 2 * kNTile * KC;
-  static constexpr size_t SMEM = 2 * STAGE_FLOATS * sizeof(float) + 4096;
+  // stages of the copy ring: as many as ~220 KB of shared memory holds (at
+  // most 4), and at most NKC + 1, so the copies run at most one tile ahead
+  static constexpr int NS_SMEM = (220 * 1024) / (STAGE_FLOATS * (int)sizeof(float));
+  static constexpr int NS_CAP = NS_SMEM < 4 ? NS_SMEM : 4;
+  static constexpr int NS = NS_CAP < NKC + 1 ? NS_CAP : NKC + 1;
+  static_assert(NS >= 2, "the copy ring needs two stages");
+  static constexpr size_t SMEM = (size_t)NS * STAGE_FLOATS * sizeof(float) + 1024;
 };
 
 // ---------------------------------------------------------------------------
@@ -261,10 +268,13 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
 // ---------------------------------------------------------------------------
 // normalised FP32 multipoles and the final rescale into FP64 L
 // ---------------------------------------------------------------------------
+// Mt_hi + Mt_lo = the normalised multipole M_n / w^n as split TF32 (the GEMM's
+// B operand, one row of KP values per cell).
 template <int P>
 __global__ void normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
                             const double *__restrict__ cmin, const double *__restrict__ cmax,
-                            const double2 *__restrict__ M, float *__restrict__ Mt) {
+                            const double2 *__restrict__ M, float *__restrict__ Mt_hi,
+                            float *__restrict__ Mt_lo) {
   using S = TcShape<P>;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells * S::KP;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -278,7 +288,9 @@ __global__ void normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
       const double2 z = M[c * S::NT + (kk >> 1)];
       v = (float)(((kk & 1) ? z.y : z.x) * pow(w, -n));
     }
-    Mt[i] = v;
+    const float h = tf32_round(v);
+    Mt_hi[i] = h;
+    Mt_lo[i] = tf32_round(v - h);
   }
 }
 
@@ -391,30 +403,56 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // ---------------------------------------------------------------------------
 // the GEMM kernel
 // ---------------------------------------------------------------------------
+// 16-byte asynchronous global -> shared copy (L2 only); with src_bytes = 0
+// the destination is zero-filled and nothing is read.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Persistent CTA over the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// The (tile, k-chunk) steps stream through an NS-stage ring: every thread
+// copies its share of the next steps' operator chunk (A, contiguous) and of
+// the gathered multipole rows (B) with cp.async, one commit group per step;
+// thread 0 issues the step's MMAs once the whole CTA has its copies, and
+// commits them to the stage's mbarrier, which the copies into that stage
+// wait for before reusing it.  The copies run up to NS - 1 steps (at most one
+// tile) ahead, so the epilogue of a tile (TMEM -> registers -> reductions into
+// Lt) overlaps the next tile's copies.  Row p of B is copied by threads p and
+// p + 128, which also fetch its source and target one tile ahead.
 template <int P>
 __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
     const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
-    const float *__restrict__ ops_lo, const float *__restrict__ Mt, float *__restrict__ Lt,
-    int *__restrict__ err) {
+    const float *__restrict__ ops_lo, const float *__restrict__ Mt_hi,
+    const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err) {
   using S = TcShape<P>;
+  constexpr int NS = S::NS;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1024-byte aligned stage buffers
   float *base = reinterpret_cast<float *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  float *stage[2];
-  stage[0] = base;
-  stage[1] = base + S::STAGE_FLOATS;
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bar_stage[NS];  // the MMAs reading a stage are done
+  __shared__ __align__(8) uint64_t bar_tile;       // all MMAs of a tile are done
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int32_t pt[kNTile], ps[kNTile];
+  __shared__ int32_t pt_buf[2][kNTile];            // targets of the tiles, by tile parity
   __shared__ int abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint64_t mask = (1ull << shift) - 1;
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int i = 0; i < NS; i++) mbar_init(&bar_stage[i], 1);
+    mbar_init(&bar_tile, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -434,108 +472,119 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
                          ((uint32_t)(128 >> 4) << 24);
   const uint32_t LBO = 128;                  // adjacent k-cores
   const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
-  uint32_t phase[2] = {0, 0};
-  bool pending[2] = {false, false};
-  bool failed = false;
 
-  for (int64_t it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
-    const TileItem item = items[it];
-    for (int i = tid; i < kNTile; i += blockDim.x) {
-      if (i < item.len) {
-        const uint64_t v = list[sorted_vals[item.start + i]];
-        pt[i] = (int)(v >> shift);
-        ps[i] = (int)(v & mask);
-      } else {
-        pt[i] = -1;
-        ps[i] = -1;
+  const int64_t ntiles = nitems > (int64_t)blockIdx.x
+                             ? (nitems - 1 - (int64_t)blockIdx.x) / gridDim.x + 1
+                             : 0;
+  const int64_t nsteps = ntiles * S::NKC;
+
+  // copy-side state of this thread: B row and half, and the tile being copied
+  const int brow = tid & (kNTile - 1), bhalf = tid >> 7;
+  int cur_src = -1, cur_cls = 0;
+  int nxt_src = -1, nxt_tgt = -1, nxt_cls = 0;
+  auto fetch = [&](int64_t jt) {  // source, target, class of row brow in local tile jt
+    nxt_src = nxt_tgt = -1;
+    nxt_cls = 0;
+    if (jt < ntiles) {
+      const TileItem it = items[(int64_t)blockIdx.x + jt * gridDim.x];
+      nxt_cls = it.cls;
+      if (brow < it.len) {
+        const uint64_t v = list[sorted_vals[it.start + brow]];
+        nxt_tgt = (int)(v >> shift);
+        nxt_src = (int)(v & mask);
       }
     }
+  };
+  auto issue_copies = [&](int64_t step) {
+    const int64_t jt = step / S::NKC;
+    const int kc = (int)(step % S::NKC);
+    if (kc == 0) {  // the copies enter tile jt
+      cur_src = nxt_src;
+      cur_cls = nxt_cls;
+      if (bhalf == 0) pt_buf[jt & 1][brow] = nxt_tgt;
+      fetch(jt + 1);
+    }
+    float *sA_hi = base + (size_t)(step % NS) * S::STAGE_FLOATS;
+    float *sA_lo = sA_hi + S::MP * S::KC;
+    float *sB_hi = sA_lo + S::MP * S::KC;
+    float *sB_lo = sB_hi + kNTile * S::KC;
+    const size_t aoff = (size_t)cur_cls * S::MP * S::KP + (size_t)kc * S::MP * S::KC;
+    for (int i = tid; i < S::MP * S::KC / 4; i += kThreadsTc) {
+      cp_async16(sA_hi + 4 * i, ops_hi + aoff + 4 * i, 16);
+      cp_async16(sA_lo + 4 * i, ops_lo + aoff + 4 * i, 16);
+    }
+    const bool have = cur_src >= 0;
+    const size_t boff = (size_t)(have ? cur_src : 0) * S::KP + (size_t)kc * S::KC;
+    const uint32_t nbytes = have ? 16u : 0u;
+#pragma unroll
+    for (int c = bhalf * (S::KC / 8); c < (bhalf + 1) * (S::KC / 8); c++) {
+      const int o = ((brow >> 3) * (S::KC / 4) + c) * 32 + (brow & 7) * 4;
+      cp_async16(sB_hi + o, Mt_hi + boff + 4 * c, nbytes);
+      cp_async16(sB_lo + o, Mt_lo + boff + 4 * c, nbytes);
+    }
+  };
+
+  fetch(0);
+  for (int64_t st = 0; st < NS - 1; st++) {
+    if (st < nsteps) issue_copies(st);
+    cp_async_commit();
+  }
+  uint32_t ph_stage = 0;  // bit i: parity of the next wait on bar_stage[i]
+  uint32_t ph_tile = 0;
+  bool failed = false;
+
+  for (int64_t step = 0; step < nsteps; step++) {
+    const int st = (int)(step % NS);
+    const int kc = (int)(step % S::NKC);
+    const int64_t jt = step / S::NKC;
+    cp_async_wait<NS - 2>();  // this thread's copies of `step` have landed
+    fence_async_smem();       // ... and are visible to the tensor core's proxy
     __syncthreads();
-    const float *ahi = ops_hi + (size_t)item.cls * S::MP * S::KP;
-    const float *alo = ops_lo + (size_t)item.cls * S::MP * S::KP;
-    for (int kc = 0; kc < S::NKC; kc++) {
-      const int b = kc & 1;
-      // the MMAs that last read this stage must be done
-      if (pending[b]) {
-        if (!mbar_wait_bounded(&bars[b], phase[b])) failed = true;
-        phase[b] ^= 1;
-        pending[b] = false;
-      }
-      float *sA_hi = stage[b];
+    if (tid == 0 && !failed) {
+      tc_fence_after();
+      float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sA_lo = sA_hi + S::MP * S::KC;
       float *sB_hi = sA_lo + S::MP * S::KC;
       float *sB_lo = sB_hi + kNTile * S::KC;
-      // A chunk: contiguous copy of the pre-laid-out operator chunk
-      {
-        const float4 *gh = reinterpret_cast<const float4 *>(ahi + (size_t)kc * S::MP * S::KC);
-        const float4 *gl = reinterpret_cast<const float4 *>(alo + (size_t)kc * S::MP * S::KC);
-        float4 *dh = reinterpret_cast<float4 *>(sA_hi);
-        float4 *dl = reinterpret_cast<float4 *>(sA_lo);
-        for (int i = tid; i < S::MP * S::KC / 4; i += blockDim.x) {
-          dh[i] = __ldg(gh + i);
-          dl[i] = __ldg(gl + i);
+      const uint32_t a_hi = smem_u32(sA_hi), a_lo = smem_u32(sA_lo);
+      const uint32_t b_hi = smem_u32(sB_hi), b_lo = smem_u32(sB_lo);
+#pragma unroll
+      for (int mt = 0; mt < S::MT; mt++) {
+        const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
+        const uint32_t d = tmem + (uint32_t)(mt * kNTile);
+#pragma unroll
+        for (int s = 0; s < S::KC / 8; s++) {
+          const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
+          const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
+          const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
+          const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
+          const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
+          const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
+          umma_tf32(d, ah, bh, idesc, acc);
+          umma_tf32(d, al, bh, idesc, 1u);
+          umma_tf32(d, ah, bl, idesc, 1u);
         }
       }
-      // B chunk: gather the sources' normalised multipoles, split hi/lo
-      for (int i = tid; i < kNTile * (S::KC / 4); i += blockDim.x) {
-        const int p = i / (S::KC / 4), cc = i % (S::KC / 4);
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        const int s = ps[p];
-        if (s >= 0)
-          v = __ldg(reinterpret_cast<const float4 *>(Mt + (size_t)s * S::KP + kc * S::KC) + cc);
-        float4 h, l;
-        h.x = tf32_round(v.x); l.x = tf32_round(v.x - h.x);
-        h.y = tf32_round(v.y); l.y = tf32_round(v.y - h.y);
-        h.z = tf32_round(v.z); l.z = tf32_round(v.z - h.z);
-        h.w = tf32_round(v.w); l.w = tf32_round(v.w - h.w);
-        const int o = ((p >> 3) * (S::KC / 4) + cc) * 32 + (p & 7) * 4;
-        *reinterpret_cast<float4 *>(sB_hi + o) = h;
-        *reinterpret_cast<float4 *>(sB_lo + o) = l;
-      }
-      fence_async_smem();
-      __syncthreads();
-      if (tid == 0 && !failed) {
-        tc_fence_after();
-        const uint32_t a_hi = smem_u32(sA_hi), a_lo = smem_u32(sA_lo);
-        const uint32_t b_hi = smem_u32(sB_hi), b_lo = smem_u32(sB_lo);
-#pragma unroll
-        for (int mt = 0; mt < S::MT; mt++) {
-          const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
-          const uint32_t d = tmem + (uint32_t)(mt * kNTile);
-#pragma unroll
-          for (int s = 0; s < S::KC / 8; s++) {
-            const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
-            const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
-            const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
-            const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
-            const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
-            const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
-            umma_tf32(d, ah, bh, idesc, acc);
-            umma_tf32(d, al, bh, idesc, 1u);
-            umma_tf32(d, ah, bl, idesc, 1u);
-          }
-        }
-        umma_commit(&bars[b]);
-      }
-      pending[b] = true;
+      umma_commit(&bar_stage[st]);
+      if (kc == S::NKC - 1) umma_commit(&bar_tile);
     }
-    // all MMAs of the tile done
-    for (int b = 0; b < 2; b++) {
-      if (pending[b]) {
-        if (!mbar_wait_bounded(&bars[b], phase[b])) failed = true;
-        phase[b] ^= 1;
-        pending[b] = false;
+    // refill the stage that step - 1 read, for step + NS - 1
+    const int64_t nstep = step + NS - 1;
+    if (nstep < nsteps) {
+      if (step >= 1) {
+        const int rs = (int)(nstep % NS);
+        if (!mbar_wait_bounded(&bar_stage[rs], (ph_stage >> rs) & 1u)) failed = true;
+        ph_stage ^= 1u << rs;
       }
+      issue_copies(nstep);
     }
-    if (failed) {
-      atomicExch(err, 1);
-      abort_sh = 1;
-    }
-    tc_fence_after();
-    __syncthreads();
-    if (abort_sh) break;
-    // epilogue: warp w reads TMEM lanes 32*(w%4).., columns of half (w/4)
-    {
+    cp_async_commit();
+    if (kc == S::NKC - 1) {
+      // epilogue of tile jt: warp w reads TMEM lanes 32*(w%4).., columns of half (w/4)
+      if (!mbar_wait_bounded(&bar_tile, ph_tile)) failed = true;
+      ph_tile ^= 1;
+      tc_fence_after();
+      const int32_t *pt = pt_buf[jt & 1];
       const int q = warp & 3, h = warp >> 2;
 #pragma unroll 1
       for (int mt = 0; mt < S::MT; mt++) {
@@ -555,10 +604,16 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
           }
         }
       }
+      tc_fence_before();
+      if (failed) {
+        atomicExch(err, 1);
+        abort_sh = 1;
+      }
+      __syncthreads();
+      if (abort_sh) break;
     }
-    tc_fence_before();
-    __syncthreads();
   }
+  cp_async_wait_all();  // no copy in flight when the CTA leaves
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
@@ -666,10 +721,10 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
     TB_LAUNCH_CHECK(ctx);
   }
   // 4. normalised multipoles, zeroed normalised locals
-  TB_CUDA(ctx, T.Mt.ensure((size_t)C * S::KP, s));
+  TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));  // hi rows, then lo rows
   TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
   normalize_M<P><<<grid_for(C * S::KP, 256, ctx->num_sms * 32), 256, 0, s>>>(
-      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p);
+      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP);
   TB_LAUNCH_CHECK(ctx);
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
   setup_timer.reset();
@@ -682,7 +737,8 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
     PhaseTimer t(ctx, &ctx->timings.m2l_tc);
     m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(
         reinterpret_cast<const TileItem *>(T.items.p), nitems, T.vals.p, ctx->m2l.p,
-        ctx->list_shift, T.ops_hi.p, T.ops_lo.p, T.Mt.p, T.Lt.p, T.err.p);
+        ctx->list_shift, T.ops_hi.p, T.ops_lo.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP, T.Lt.p,
+        T.err.p);
     TB_LAUNCH_CHECK(ctx);
   }
   add_scaled_L<P><<<grid_for(C * S::NT, 256, ctx->num_sms * 32), 256, 0, s>>>(
