@@ -19,14 +19,16 @@
 //  3. per tensor-core class the real K x K operator is built in FP64 from the
 //     unit-width singular harmonics and split into TF32 hi + lo parts, laid
 //     out as K-major core matrices (8 rows x 16 bytes) ready for smem.
-//  4. GEMM kernel: a CTA takes tiles of 128 pairs of one class; K is streamed
-//     in chunks through a 2-4 stage shared-memory ring filled by cp.async
-//     (operator chunks and the pre-split multipole rows); one thread issues
-//     tcgen05.mma kind::tf32 (M=128 rows of T per M-tile, N=128 pairs, K=8)
-//     three times per k-step (hi*hi + lo*hi + hi*lo: split-precision
-//     "3xTF32", FP32 accumulation in TMEM); completion via tcgen05.commit to
-//     an mbarrier (bounded waits); the epilogue reads TMEM with tcgen05.ld and
-//     adds each column into its target's Lt with fire-and-forget reductions.
+//  4. GEMM kernel, warp-specialised: a CTA takes tiles of 128 pairs of one
+//     class; producer warps stream the operator's K chunks (bulk copies) and
+//     the sources' pre-split multipole rows (cp.async) through a 2-4 stage
+//     shared-memory ring; one thread issues tcgen05.mma kind::tf32 (M=128 rows
+//     of T per M-tile, N=128 pairs, K=8) three times per k-step (hi*hi +
+//     lo*hi + hi*lo: split-precision "3xTF32", FP32 accumulation in TMEM);
+//     epilogue warps read the finished accumulator with tcgen05.ld and add
+//     each column into its target's Lt with fire-and-forget reductions, while
+//     the next tile accumulates in the second TMEM buffer.  All hand-offs are
+//     mbarriers with bounded waits.
 //  5. Lt is rescaled and added into the FP64 L.
 #include <algorithm>
 #include <optional>
@@ -41,7 +43,6 @@ namespace {
 
 constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor cores
 constexpr int kNTile = 128;        // pairs per tile (MMA N)
-constexpr int kThreadsTc = 256;    // 8 warps
 constexpr uint64_t kKeyEmpty = 0xFFFFFFFFFFFFull;  // source has no bodies: no work
 constexpr uint64_t kKeyRare = 0xFFFFFFFFFFFEull;   // offset outside the key range: FP64
 constexpr int kOffBias = 8192;
@@ -55,7 +56,10 @@ struct TcShape {
   static constexpr int KC = MT <= 2 ? 32 : 16;        // K chunk per stage
   static constexpr int KP = ((K + KC - 1) / KC) * KC; // padded K
   static constexpr int NKC = KP / KC;
-  static constexpr int TMEM_COLS = MT == 1 ? 128 : (MT == 2 ? 256 : 512);
+  // TMEM accumulators: two (double-buffered epilogue) when they fit in the
+  // 512 columns, else one
+  static constexpr int TBUF = 2 * MT * 128 <= 512 ? 2 : 1;
+  static constexpr int TMEM_COLS = TBUF * MT * 128 <= 256 ? 256 : 512;
   // one stage: A hi/lo (MP x KC) + B hi/lo (128 x KC) floats
   static constexpr int STAGE_FLOATS = 2 * MP * KC + 2 * kNTile * KC;
   // stages of the copy ring: as many as ~220 KB of shared memory holds (at
@@ -410,27 +414,103 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t 
                "r"(src_bytes)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// Arrive on `bar` once all of this thread's earlier cp.async copies have landed
+// (the barrier's expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
+// Bulk copy of `bytes` (a multiple of 16) global -> shared, completing on `bar`.
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Wait for the phase of `bar` with the given parity; gives up (false) when
+// another role has raised *abort or after about 2 s, then raising *abort.
+__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volatile int *abort) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort) return false;
+    if (clock64() - t0 > 4000000000LL) {
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
 
-// Persistent CTA over the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
-// The (tile, k-chunk) steps stream through an NS-stage ring: every thread
-// copies its share of the next steps' operator chunk (A, contiguous) and of
-// the gathered multipole rows (B) with cp.async, one commit group per step;
-// thread 0 issues the step's MMAs once the whole CTA has its copies, and
-// commits them to the stage's mbarrier, which the copies into that stage
-// wait for before reusing it.  The copies run up to NS - 1 steps (at most one
-// tile) ahead, so the epilogue of a tile (TMEM -> registers -> reductions into
-// Lt) overlaps the next tile's copies.  Row p of B is copied by threads p and
-// p + 128, which also fetch its source and target one tile ahead.
+// MMAs of one k-chunk: for each M-tile, KC/8 k-steps of three tf32 MMAs
+// (hi*hi, lo*hi, hi*lo) into TMEM columns dcol + [mt*128, mt*128+128).
+// a_hi/a_lo point at the chunk's operator rows (core-matrix layout), b_hi/b_lo
+// at the chunk's 128 multipole rows.
+template <int P>
+__device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, uint32_t a_lo,
+                                                 uint32_t b_hi, uint32_t b_lo, int kc) {
+  using S = TcShape<P>;
+  // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
+                         ((uint32_t)(128 >> 4) << 24);
+  const uint32_t LBO = 128;                  // adjacent k-cores
+  const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
+#pragma unroll
+  for (int mt = 0; mt < S::MT; mt++) {
+    const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
+    const uint32_t d = dcol + (uint32_t)(mt * kNTile);
+#pragma unroll
+    for (int s = 0; s < S::KC / 8; s++) {
+      const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
+      const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
+      const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
+      const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
+      const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
+      const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
+      umma_tf32(d, ah, bh, idesc, acc);
+      umma_tf32(d, al, bh, idesc, 1u);
+      umma_tf32(d, ah, bl, idesc, 1u);
+    }
+  }
+}
+
+// Warp roles of the GEMM kernel.
+constexpr int kProdThreads = 256;  // warps 0-7: copies into the stage ring
+constexpr int kEpiWarp0 = 8;       // warps 8-15: epilogue (TMEM lane quarter warp % 4,
+constexpr int kEpiWarps = 8;       //   column half (warp - 8) / 4)
+constexpr int kMmaWarp = 16;       // warp 16: TMEM allocation, MMA issue (lane 0)
+constexpr int kThreadsTc = 32 * 17;
+
+// Persistent CTA over the tiles blockIdx.x, blockIdx.x + gridDim.x, ...,
+// warp-specialised; the roles meet only at mbarriers:
+//  - producers (warps 0-7) walk the (tile, k-chunk) steps through an NS-stage
+//    ring: thread 0 bulk-copies the step's operator chunk (A, contiguous, hi
+//    and lo); every producer cp.async-copies its share of the 128 gathered
+//    multipole rows (B, pre-split hi/lo; lanes of a warp cover whole row
+//    segments) and arrives on full[stage] once they
+//    have landed.  A stage is refilled after the MMAs that read it commit to
+//    empty[stage].
+//  - the MMA thread (warp 16, lane 0) waits for full[stage], issues the
+//    chunk's 3xTF32 MMAs into one of TBUF TMEM accumulators and commits them
+//    to empty[stage]; after a tile's last chunk it commits to tfull[buffer].
+//  - the epilogue warps (8-15) wait for tfull[buffer], read the accumulator
+//    with tcgen05.ld and add column j into row target(j) of Lt, then arrive on
+//    tempty[buffer], which the MMA thread waits for before reusing it; with
+//    two TMEM buffers the epilogue of tile i overlaps the MMAs of tile i+1.
+// Every wait is bounded and also gives up when another role has aborted; the
+// CTA then drains its copies and its MMAs before freeing TMEM.
 template <int P>
 __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
@@ -439,26 +519,33 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err) {
   using S = TcShape<P>;
   constexpr int NS = S::NS;
+  constexpr int NB = S::TBUF;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   float *base = reinterpret_cast<float *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t bar_stage[NS];  // the MMAs reading a stage are done
-  __shared__ __align__(8) uint64_t bar_tile;       // all MMAs of a tile are done
-  __shared__ uint32_t tmem_base_sh;
-  __shared__ int32_t pt_buf[2][kNTile];            // targets of the tiles, by tile parity
+  __shared__ __align__(8) uint64_t full[NS], empty[NS], tfull[2], tempty[2], fin;
+  __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
+  volatile int *abort = &abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint64_t mask = (1ull << shift) - 1;
   if (tid == 0) {
-    for (int i = 0; i < NS; i++) mbar_init(&bar_stage[i], 1);
-    mbar_init(&bar_tile, 1);
+    for (int i = 0; i < NS; i++) {
+      mbar_init(&full[i], kProdThreads + 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], kEpiWarps);
+    }
+    mbar_init(&fin, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(&tmem_base_sh)),
+                     smem_u32(&tmem_sh)),
                  "r"((uint32_t)S::TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -466,156 +553,175 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tmem_base_sh;
-  // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
-  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
-                         ((uint32_t)(128 >> 4) << 24);
-  const uint32_t LBO = 128;                  // adjacent k-cores
-  const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
+  const uint32_t tmem = tmem_sh;
 
   const int64_t ntiles = nitems > (int64_t)blockIdx.x
                              ? (nitems - 1 - (int64_t)blockIdx.x) / gridDim.x + 1
                              : 0;
   const int64_t nsteps = ntiles * S::NKC;
+  auto item_of = [&](int64_t jt) { return items[(int64_t)blockIdx.x + jt * gridDim.x]; };
 
-  // copy-side state of this thread: B row and half, and the tile being copied
-  const int brow = tid & (kNTile - 1), bhalf = tid >> 7;
-  int cur_src = -1, cur_cls = 0;
-  int nxt_src = -1, nxt_tgt = -1, nxt_cls = 0;
-  auto fetch = [&](int64_t jt) {  // source, target, class of row brow in local tile jt
-    nxt_src = nxt_tgt = -1;
-    nxt_cls = 0;
-    if (jt < ntiles) {
-      const TileItem it = items[(int64_t)blockIdx.x + jt * gridDim.x];
-      nxt_cls = it.cls;
-      if (brow < it.len) {
-        const uint64_t v = list[sorted_vals[it.start + brow]];
-        nxt_tgt = (int)(v >> shift);
-        nxt_src = (int)(v & mask);
+  if (warp < kEpiWarp0) {
+    // ---------------- producers ----------------
+    // B: each row chunk is KC floats = PPR 16-byte pieces; PPR consecutive
+    // lanes copy one row's chunk, so a warp instruction reads whole 128-byte
+    // (or 64-byte) row segments.  Thread t copies piece t % PPR of rows
+    // t / PPR + i * RPP (RPP = rows per pass of all producers, i < NRT) and
+    // fetches their sources and the tile's class one tile ahead.
+    constexpr int PPR = S::KC / 4;
+    constexpr int RPP = kProdThreads / PPR;
+    constexpr int NRT = kNTile / RPP;
+    const int bpiece = tid % PPR, brow0 = tid / PPR;
+    int cur_src[NRT], nxt_src[NRT];
+    int cur_cls = 0, nxt_cls = 0;
+    auto fetch = [&](int64_t jt) {
+      nxt_cls = 0;
+      TileItem it;
+      it.len = 0;
+      it.start = 0;
+      if (jt < ntiles) {
+        it = item_of(jt);
+        nxt_cls = it.cls;
       }
-    }
-  };
-  auto issue_copies = [&](int64_t step) {
-    const int64_t jt = step / S::NKC;
-    const int kc = (int)(step % S::NKC);
-    if (kc == 0) {  // the copies enter tile jt
-      cur_src = nxt_src;
-      cur_cls = nxt_cls;
-      if (bhalf == 0) pt_buf[jt & 1][brow] = nxt_tgt;
-      fetch(jt + 1);
-    }
-    float *sA_hi = base + (size_t)(step % NS) * S::STAGE_FLOATS;
-    float *sA_lo = sA_hi + S::MP * S::KC;
-    float *sB_hi = sA_lo + S::MP * S::KC;
-    float *sB_lo = sB_hi + kNTile * S::KC;
-    const size_t aoff = (size_t)cur_cls * S::MP * S::KP + (size_t)kc * S::MP * S::KC;
-    for (int i = tid; i < S::MP * S::KC / 4; i += kThreadsTc) {
-      cp_async16(sA_hi + 4 * i, ops_hi + aoff + 4 * i, 16);
-      cp_async16(sA_lo + 4 * i, ops_lo + aoff + 4 * i, 16);
-    }
-    const bool have = cur_src >= 0;
-    const size_t boff = (size_t)(have ? cur_src : 0) * S::KP + (size_t)kc * S::KC;
-    const uint32_t nbytes = have ? 16u : 0u;
 #pragma unroll
-    for (int c = bhalf * (S::KC / 8); c < (bhalf + 1) * (S::KC / 8); c++) {
-      const int o = ((brow >> 3) * (S::KC / 4) + c) * 32 + (brow & 7) * 4;
-      cp_async16(sB_hi + o, Mt_hi + boff + 4 * c, nbytes);
-      cp_async16(sB_lo + o, Mt_lo + boff + 4 * c, nbytes);
-    }
-  };
-
-  fetch(0);
-  for (int64_t st = 0; st < NS - 1; st++) {
-    if (st < nsteps) issue_copies(st);
-    cp_async_commit();
-  }
-  uint32_t ph_stage = 0;  // bit i: parity of the next wait on bar_stage[i]
-  uint32_t ph_tile = 0;
-  bool failed = false;
-
-  for (int64_t step = 0; step < nsteps; step++) {
-    const int st = (int)(step % NS);
-    const int kc = (int)(step % S::NKC);
-    const int64_t jt = step / S::NKC;
-    cp_async_wait<NS - 2>();  // this thread's copies of `step` have landed
-    fence_async_smem();       // ... and are visible to the tensor core's proxy
-    __syncthreads();
-    if (tid == 0 && !failed) {
-      tc_fence_after();
+      for (int i = 0; i < NRT; i++) {
+        const int row = brow0 + i * RPP;
+        nxt_src[i] = row < it.len ? (int)(list[sorted_vals[it.start + row]] & mask) : -1;
+      }
+    };
+    fetch(0);
+    int64_t issued = 0;
+    for (int64_t step = 0; step < nsteps; step++) {
+      const int st = (int)(step % NS);
+      if (step >= NS && !wait_phase(&empty[st], (uint32_t)((step / NS - 1) & 1), abort)) break;
+      const int64_t jt = step / S::NKC;
+      const int kc = (int)(step % S::NKC);
+      if (kc == 0) {
+#pragma unroll
+        for (int i = 0; i < NRT; i++) cur_src[i] = nxt_src[i];
+        cur_cls = nxt_cls;
+        fetch(jt + 1);
+      }
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sA_lo = sA_hi + S::MP * S::KC;
       float *sB_hi = sA_lo + S::MP * S::KC;
       float *sB_lo = sB_hi + kNTile * S::KC;
-      const uint32_t a_hi = smem_u32(sA_hi), a_lo = smem_u32(sA_lo);
-      const uint32_t b_hi = smem_u32(sB_hi), b_lo = smem_u32(sB_lo);
+      if (tid == 0) {
+        const size_t aoff = (size_t)cur_cls * S::MP * S::KP + (size_t)kc * S::MP * S::KC;
+        const uint32_t abytes = (uint32_t)(S::MP * S::KC * sizeof(float));
+        mbar_expect_tx(&full[st], 2 * abytes);
+        bulk_copy(sA_hi, ops_hi + aoff, abytes, &full[st]);
+        bulk_copy(sA_lo, ops_lo + aoff, abytes, &full[st]);
+      }
 #pragma unroll
-      for (int mt = 0; mt < S::MT; mt++) {
-        const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
-        const uint32_t d = tmem + (uint32_t)(mt * kNTile);
-#pragma unroll
-        for (int s = 0; s < S::KC / 8; s++) {
-          const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
-          const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
-          const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
-          const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
-          const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
-          const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
-          umma_tf32(d, ah, bh, idesc, acc);
-          umma_tf32(d, al, bh, idesc, 1u);
-          umma_tf32(d, ah, bl, idesc, 1u);
+      for (int i = 0; i < NRT; i++) {
+        const int row = brow0 + i * RPP;
+        const bool have = cur_src[i] >= 0;
+        const size_t boff = (size_t)(have ? cur_src[i] : 0) * S::KP + (size_t)kc * S::KC +
+                            4 * bpiece;
+        const int o = ((row >> 3) * PPR + bpiece) * 32 + (row & 7) * 4;
+        cp_async16(sB_hi + o, Mt_hi + boff, have ? 16u : 0u);
+        cp_async16(sB_lo + o, Mt_lo + boff, have ? 16u : 0u);
+      }
+      cp_async_arrive_noinc(&full[st]);
+      issued = step + 1;
+    }
+    cp_async_wait_all();
+    if (tid == 0 && *abort) {
+      // bulk copies of steps the MMA thread may not have consumed: let them land
+      for (int64_t s = issued > NS ? issued - NS : 0; s < issued; s++) {
+        const long long t0 = clock64();
+        while (!mbar_try_wait(&full[s % NS], (uint32_t)((s / NS) & 1)) &&
+               clock64() - t0 < 200000000LL) {
         }
       }
-      umma_commit(&bar_stage[st]);
-      if (kc == S::NKC - 1) umma_commit(&bar_tile);
     }
-    // refill the stage that step - 1 read, for step + NS - 1
-    const int64_t nstep = step + NS - 1;
-    if (nstep < nsteps) {
-      if (step >= 1) {
-        const int rs = (int)(nstep % NS);
-        if (!mbar_wait_bounded(&bar_stage[rs], (ph_stage >> rs) & 1u)) failed = true;
-        ph_stage ^= 1u << rs;
+  } else if (warp == kMmaWarp) {
+    // ---------------- MMA issue ----------------
+    if (lane == 0) {
+      for (int64_t jt = 0; jt < ntiles && !*abort; jt++) {
+        const int b = NB == 2 ? (int)(jt & 1) : 0;
+        const int64_t use_b = NB == 2 ? (jt >> 1) : jt;
+        if (use_b >= 1 && !wait_phase(&tempty[b], (uint32_t)((use_b - 1) & 1), abort)) break;
+        tc_fence_after();
+        const uint32_t dcol = tmem + (uint32_t)(b * S::MT * kNTile);
+        bool ok = true;
+        for (int kc = 0; kc < S::NKC; kc++) {
+          const int64_t step = jt * S::NKC + kc;
+          const int st = (int)(step % NS);
+          if (!wait_phase(&full[st], (uint32_t)((step / NS) & 1), abort)) {
+            ok = false;
+            break;
+          }
+          fence_async_smem();  // the cp.async rows are visible to the tensor core
+          tc_fence_after();
+          float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
+          float *sA_lo = sA_hi + S::MP * S::KC;
+          float *sB_hi = sA_lo + S::MP * S::KC;
+          float *sB_lo = sB_hi + kNTile * S::KC;
+          issue_chunk_mmas<P>(dcol, smem_u32(sA_hi), smem_u32(sA_lo), smem_u32(sB_hi),
+                              smem_u32(sB_lo), kc);
+          umma_commit(&empty[st]);
+        }
+        if (!ok) break;
+        umma_commit(&tfull[b]);
       }
-      issue_copies(nstep);
+      // every MMA issued so far has completed before TMEM is freed
+      umma_commit(&fin);
+      const long long t0 = clock64();
+      while (!mbar_try_wait(&fin, 0) && clock64() - t0 < 400000000LL) {
+      }
     }
-    cp_async_commit();
-    if (kc == S::NKC - 1) {
-      // epilogue of tile jt: warp w reads TMEM lanes 32*(w%4).., columns of half (w/4)
-      if (!mbar_wait_bounded(&bar_tile, ph_tile)) failed = true;
-      ph_tile ^= 1;
+    __syncwarp();
+  } else {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3;                   // TMEM lane quarter of this warp (warp % 4)
+    const int h = (warp - kEpiWarp0) >> 2;    // column half
+    int tg[2], tg_next[2];   // targets of columns 64h + 32c + lane, this tile and the next
+    auto load_targets = [&](int64_t jt, int (&t)[2]) {
+      TileItem it;
+      it.len = 0;
+      it.start = 0;
+      if (jt < ntiles) it = item_of(jt);
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int col = h * 64 + c * 32 + lane;
+        t[c] = col < it.len ? (int)(list[sorted_vals[it.start + col]] >> shift) : -1;
+      }
+    };
+    load_targets(0, tg_next);
+    for (int64_t jt = 0; jt < ntiles; jt++) {
+      const int b = NB == 2 ? (int)(jt & 1) : 0;
+      const int64_t use_b = NB == 2 ? (jt >> 1) : jt;
+#pragma unroll
+      for (int c = 0; c < 2; c++) tg[c] = tg_next[c];
+      load_targets(jt + 1, tg_next);
+      if (!wait_phase(&tfull[b], (uint32_t)(use_b & 1), abort)) break;
       tc_fence_after();
-      const int32_t *pt = pt_buf[jt & 1];
-      const int q = warp & 3, h = warp >> 2;
 #pragma unroll 1
       for (int mt = 0; mt < S::MT; mt++) {
         const int r = mt * 128 + q * 32 + lane;
-#pragma unroll 1
-        for (int cchunk = 0; cchunk < 2; cchunk++) {
-          const int col0 = h * 64 + cchunk * 32;
-          uint32_t v[32];
-          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(mt * kNTile + col0);
-          tmem_ld32(taddr, v);
-          if (r < S::K) {
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-              const int t = pt[col0 + j];
-              if (t >= 0) atomicAdd(Lt + (size_t)t * S::KP + r, __uint_as_float(v[j]));
-            }
+        for (int c = 0; c < 2; c++) {
+          uint32_t v[32];
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
+                                 (uint32_t)(b * S::MT * kNTile + mt * kNTile + h * 64 + c * 32);
+          tmem_ld32(taddr, v);
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int t = __shfl_sync(0xffffffffu, tg[c], j);
+            if (t >= 0 && r < S::K) atomicAdd(Lt + (size_t)t * S::KP + r, __uint_as_float(v[j]));
           }
         }
       }
       tc_fence_before();
-      if (failed) {
-        atomicExch(err, 1);
-        abort_sh = 1;
-      }
-      __syncthreads();
-      if (abort_sh) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
     }
   }
-  cp_async_wait_all();  // no copy in flight when the CTA leaves
   __syncthreads();
-  if (warp == 0) {
+  if (tid == 0 && abort_sh) atomicExch(err, 1);
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"((uint32_t)S::TMEM_COLS)
@@ -731,14 +837,16 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   // 5. FP64 part (rare classes) writes L; the GEMM adds into Lt
   TB_TRY(m2l_fp64_masked(ctx, T.use64.p));
   if (nitems > 0) {
-    TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)S::SMEM));
-    const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
     PhaseTimer t(ctx, &ctx->timings.m2l_tc);
-    m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(
-        reinterpret_cast<const TileItem *>(T.items.p), nitems, T.vals.p, ctx->m2l.p,
-        ctx->list_shift, T.ops_hi.p, T.ops_lo.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP, T.Lt.p,
-        T.err.p);
+    const float *mt_hi = T.Mt.p, *mt_lo = T.Mt.p + (size_t)C * S::KP;
+    const TileItem *it = reinterpret_cast<const TileItem *>(T.items.p);
+    const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
+    static_assert(S::SMEM <= 227 * 1024 - 4096, "shared memory");
+    TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+    m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(it, nitems, T.vals.p, ctx->m2l.p,
+                                                        ctx->list_shift, T.ops_hi.p, T.ops_lo.p,
+                                                        mt_hi, mt_lo, T.Lt.p, T.err.p);
     TB_LAUNCH_CHECK(ctx);
   }
   add_scaled_L<P><<<grid_for(C * S::NT, 256, ctx->num_sms * 32), 256, 0, s>>>(
