@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
       double rhon = rhom;
 #pragma unroll
       for (int n = m; n < P; n++) {
-        if (n > m) rhon /= -(n + m);
+        if (n > m) rhon *= 1.0 / -(n + m);  // constants after unrolling
         const double sc = q * rhon * p;
         double vx = sc * eim.x, vy = -sc * eim.y;
 #pragma unroll
@@ -88,11 +88,11 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
         } else {
           const double p2 = p1;
           p1 = p;
-          p = (x * (2 * n + 1) * p1 - (n + m) * p2) / (n - m + 1);
+          p = (x * (2 * n + 1) * p1 - (n + m) * p2) * (1.0 / (n - m + 1));
           rhon *= rho;
         }
       }
-      rhom = rhom * rho / (double)(-(2 * m + 2) * (2 * m + 1));
+      rhom = rhom * rho * (1.0 / (double)(-(2 * m + 2) * (2 * m + 1)));
       pn = -pn * fact * y;
       fact += 2;
       eim = cmul(eim, ei);
@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
     double r, theta, phi;
     cart2sph(sx[bi] - cx, sy[bi] - cy, sz[bi] - cz, r, theta, phi);
     const double x = cos(theta), y = sin(theta);
+    const double inv_y = 1.0 / y, inv_r = 1.0 / r;
     double sp, cp;
     sincos(phi, &sp, &cp);
     const cd ei{cp, sp};
@@ -346,16 +347,16 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
         if (n == m) {
           const double pnew = x * (2 * m + 1) * p1;
           ys = rhom * p;
-          yts = rhom * (pnew - (m + 1) * x * p1) / y;
+          yts = rhom * (pnew - (m + 1) * x * p1) * inv_y;
           p = pnew;
           rhon = rhom * r;
         } else {
-          rhon /= -(n + m);
+          rhon *= 1.0 / -(n + m);  // constants after unrolling
           ys = rhon * p;
           const double p2 = p1;
           p1 = p;
-          p = (x * (2 * n + 1) * p1 - (n + m) * p2) / (n - m + 1);
-          yts = rhon * ((n - m + 1) * p - (n + 1) * x * p1) / y;
+          p = (x * (2 * n + 1) * p1 - (n + m) * p2) * (1.0 / (n - m + 1));
+          yts = rhon * ((n - m + 1) * p - (n + 1) * x * p1) * inv_y;
           rhon *= r;
         }
         const cd Lv = Lc[n * (n + 1) / 2 + m];
@@ -363,11 +364,11 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
         const cd LYt = cmul(Lv, scal(yts, eim));
         const double f = (m == 0) ? 1.0 : 2.0;
         pot += f * LY.x;
-        s0 += f * LY.x / r * n;
+        s0 += f * LY.x * inv_r * n;
         s1 += f * LYt.x;
         if (m > 0) s2 += 2 * (-LY.y) * m;  // real(L*Y*i) = -imag(L*Y)
       }
-      rhom = rhom * r / (double)(-(2 * m + 2) * (2 * m + 1));
+      rhom = rhom * r * (1.0 / (double)(-(2 * m + 2) * (2 * m + 1)));
       pn = -pn * fact * y;
       fact += 2;
       eim = cmul(eim, ei);

@@ -23,6 +23,18 @@ __device__ __forceinline__ void cmac(cd &acc, cd a, cd b) {
 }
 __device__ __forceinline__ double oddeven(int n) { return (n & 1) ? -1.0 : 1.0; }
 
+// 1/i for small integers 0 < i < 64: the recurrences below multiply by these
+// instead of dividing (an FP64 division is a long instruction sequence); the
+// results differ from exact division by at most an ulp per step.
+struct RecipTable {
+  double v[64];
+  constexpr RecipTable() : v() {
+    for (int i = 1; i < 64; i++) v[i] = 1.0 / i;
+  }
+};
+static __constant__ RecipTable kRecip = RecipTable();
+__device__ __forceinline__ double recip(int i) { return kRecip.v[i]; }
+
 // cart2sph (ex/LaplaceSphericalCPU_tapas.h:43-47)
 __device__ __forceinline__ void cart2sph(double dx, double dy, double dz, double &r,
                                          double &theta, double &phi) {
@@ -41,7 +53,7 @@ __device__ __forceinline__ void multipole_column(int m, double rho, double x, do
   cd eim{1.0, 0.0};
   for (int k = 0; k < m; k++) {
     rhom *= rho;
-    rhom /= -(2 * k + 2) * (2 * k + 1);
+    rhom *= -recip(2 * k + 2) * recip(2 * k + 1);
     pn = -pn * fact * y;
     fact += 2;
     eim = cmul(eim, ei);
@@ -54,13 +66,13 @@ __device__ __forceinline__ void multipole_column(int m, double rho, double x, do
   p = x * (2 * m + 1) * p1;
   double rhon = rhom * rho;
   for (int n = m + 1; n < P; n++) {
-    rhon /= -(n + m);
+    rhon *= -recip(n + m);
     cd w = scal(rhon * p, eim);
     Y[n * n + n + m] = w;
     Y[n * n + n - m] = conjd(w);
     double p2 = p1;
     p1 = p;
-    p = (x * (2 * n + 1) * p1 - (n + m) * p2) / (n - m + 1);
+    p = (x * (2 * n + 1) * p1 - (n + m) * p2) * recip(n - m + 1);
     rhon *= rho;
   }
 }
@@ -91,7 +103,7 @@ __device__ __forceinline__ void local_column(int m, double rho, double x, double
     Y[n * n + n - m] = conjd(w);
     double p2 = p1;
     p1 = p;
-    p = (x * (2 * n + 1) * p1 - (n + m) * p2) / (n - m + 1);
+    p = (x * (2 * n + 1) * p1 - (n + m) * p2) * recip(n - m + 1);
     rhon *= invR * (n - m + 1);
   }
 }
