@@ -24,6 +24,9 @@
 // and the FP64 centre difference, so the separation x_i - x_j is formed from
 // ~47-bit operands and rounds once.  1/r is the hardware rsqrt (its error is far below
 // the near field's summation error, so no Newton step).
+// A source leaf whose box lies at least one target-leaf width away from the
+// target's box (every pair at least that far apart) skips the lo parts: one
+// rounding of a coordinate is then <= ~2e-7 of the separation.
 // Each source leaf is summed in plain FP32 and the partial is Kahan-added into
 // the target's (sum, compensation) pair; the final near field is FP64.
 #include <algorithm>
@@ -238,6 +241,7 @@ struct __align__(16) SrcRec {
 // target leaf (FP64 difference as FP32 hi + lo).
 struct __align__(16) LeafMeta {
   int b0, ns;
+  int far;  // the leaf's box is at least one target-leaf width from the target's
   float hx, hy, hz, lx, ly, lz;
 };
 
@@ -253,9 +257,11 @@ struct __align__(16) LeafMeta {
 template <int kR>
 __device__ __forceinline__ void mixed_tile(
     int lane, int wi, int tb0, int nt, int L, int G, int e0, int e1, double tcx, double tcy,
-    double tcz, const uint64_t *__restrict__ list, uint64_t mask, const int32_t *__restrict__ cbeg,
-    const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
-    const float4 *__restrict__ rel_hi, const float4 *__restrict__ rel_lo, SrcRec (*ss)[kStage],
+    double tcz, double tw, const uint64_t *__restrict__ list, uint64_t mask,
+    const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
+    const double *__restrict__ ccen, const double *__restrict__ cmin,
+    const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
+    const float4 *__restrict__ rel_lo, SrcRec (*ss)[kStage],
     LeafMeta (*mt)[32], double4 (*red)[32], double *__restrict__ trg) {
   const int g = lane / L, tl = lane - g * L;
   const bool active = g < G;
@@ -288,6 +294,10 @@ __device__ __forceinline__ void mixed_tile(
                    dcz = ccen[3 * s + 2] - tcz;
       m.hx = (float)dcx; m.hy = (float)dcy; m.hz = (float)dcz;
       m.lx = (float)(dcx - m.hx); m.ly = (float)(dcy - m.hy); m.lz = (float)(dcz - m.hz);
+      // boxes separated by >= tw along some axis: every pair is >= tw apart
+      const double half = 0.5 * (tw + (cmax[3 * s] - cmin[3 * s]));
+      const double gap = fmax(fabs(dcx), fmax(fabs(dcy), fabs(dcz))) - half;
+      m.far = gap >= tw ? 1 : 0;
       meta[lane] = m;
     }
     __syncwarp();
@@ -308,14 +318,19 @@ __device__ __forceinline__ void mixed_tile(
     while (j < nbat) {
       const int cnt = min(kStage, ns_j - ch);
       __syncwarp();
+      const bool far = meta[j].far != 0;
       if (lane < cnt) {
         const LeafMeta &m = meta[j];
         float ex, ey, ez;
         const float ax = two_sum(ph.x, m.hx, ex), ay = two_sum(ph.y, m.hy, ey),
                     az = two_sum(ph.z, m.hz, ez);
-        ss[wi][lane].hi = make_float4(ax, ay, az, ph.w);
-        ss[wi][lane].lo =
-            make_float4(ex + (pl.x + m.lx), ey + (pl.y + m.ly), ez + (pl.z + m.lz), 0.f);
+        const float lx = ex + (pl.x + m.lx), ly = ey + (pl.y + m.ly), lz = ez + (pl.z + m.lz);
+        if (far) {  // one float per coordinate, rounded once
+          ss[wi][lane].hi = make_float4(ax + lx, ay + ly, az + lz, ph.w);
+        } else {
+          ss[wi][lane].hi = make_float4(ax, ay, az, ph.w);
+          ss[wi][lane].lo = make_float4(lx, ly, lz, 0.f);
+        }
       }
       __syncwarp();
       // next chunk: the rest of this leaf, else the next non-empty leaf of the batch
@@ -333,24 +348,46 @@ __device__ __forceinline__ void mixed_tile(
           pl = rel_lo[b0 + ch2 + lane];
         }
       }
-      // two sources in flight: their rsqrt latencies overlap
+      if (far) {
+        // separations >= the target leaf's width: plain FP32 coordinates in the
+        // target frame (relative error of a separation <= ~2e-7), no r = 0 case
 #pragma unroll 2
-      for (int k = gs; k < cnt; k += G) {
-        const float4 bh = ss[wi][k].hi;
-        const float4 bl = ss[wi][k].lo;
+        for (int k = gs; k < cnt; k += G) {
+          const float4 bh = ss[wi][k].hi;
 #pragma unroll
-        for (int r = 0; r < kR; r++) {
-          const float dx = (txh[r] - bh.x) + (txl[r] - bl.x);
-          const float dy = (tyh[r] - bh.y) + (tyl[r] - bl.y);
-          const float dz = (tzh[r] - bh.z) + (tzl[r] - bl.z);
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const float ri = r2 >= FLT_MIN ? rsqrt_ftz(r2) : 0.f;
-          const float qr = bh.w * ri;
-          const float qr3 = qr * ri * ri;
-          tp[r] += qr;
-          tx[r] = fmaf(dx, qr3, tx[r]);
-          ty[r] = fmaf(dy, qr3, ty[r]);
-          tz[r] = fmaf(dz, qr3, tz[r]);
+          for (int r = 0; r < kR; r++) {
+            const float dx = txh[r] - bh.x, dy = tyh[r] - bh.y, dz = tzh[r] - bh.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float ri = rsqrt_ftz(r2);
+            const float qr = bh.w * ri;
+            const float qr3 = qr * ri * ri;
+            tp[r] += qr;
+            tx[r] = fmaf(dx, qr3, tx[r]);
+            ty[r] = fmaf(dy, qr3, ty[r]);
+            tz[r] = fmaf(dz, qr3, tz[r]);
+          }
+        }
+      } else {
+        // touching or nearby leaves: separations from (hi, lo) coordinates
+        // two sources in flight: their rsqrt latencies overlap
+#pragma unroll 2
+        for (int k = gs; k < cnt; k += G) {
+          const float4 bh = ss[wi][k].hi;
+          const float4 bl = ss[wi][k].lo;
+#pragma unroll
+          for (int r = 0; r < kR; r++) {
+            const float dx = (txh[r] - bh.x) + (txl[r] - bl.x);
+            const float dy = (tyh[r] - bh.y) + (tyl[r] - bl.y);
+            const float dz = (tzh[r] - bh.z) + (tzl[r] - bl.z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float ri = r2 >= FLT_MIN ? rsqrt_ftz(r2) : 0.f;
+            const float qr = bh.w * ri;
+            const float qr3 = qr * ri * ri;
+            tp[r] += qr;
+            tx[r] = fmaf(dx, qr3, tx[r]);
+            ty[r] = fmaf(dy, qr3, ty[r]);
+            tz[r] = fmaf(dz, qr3, tz[r]);
+          }
         }
       }
       if (leaf_done) {
@@ -393,7 +430,8 @@ __global__ void __launch_bounds__(kMixedThreads, kMixedBlocks) p2p_mixed_kernel(
     const uint32_t *__restrict__ order, int64_t nleaves, int *__restrict__ counter,
     const int32_t *__restrict__ off, const uint64_t *__restrict__ list, uint64_t src_mask,
     const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
-    const double *__restrict__ ccen, const float4 *__restrict__ rel_hi,
+    const double *__restrict__ ccen, const double *__restrict__ cmin,
+    const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
     const float4 *__restrict__ rel_lo, double *__restrict__ trg) {
   __shared__ SrcRec ss[kMixedWarps][kStage];
   __shared__ LeafMeta mt[kMixedWarps][32];
@@ -406,13 +444,14 @@ __global__ void __launch_bounds__(kMixedThreads, kMixedBlocks) p2p_mixed_kernel(
     const int tb0 = cbeg[c], nt_all = cnb[c];
     const int e0 = off[c], e1 = off[c + 1];
     const double tcx = ccen[3 * c], tcy = ccen[3 * c + 1], tcz = ccen[3 * c + 2];
+    const double tw = cmax[3 * c] - cmin[3 * c];
     for (int tbase = 0; tbase < nt_all; tbase += 32 * kMaxR) {
       const int nt = min(nt_all - tbase, 32 * kMaxR);
       int R, L, G;
       mixed_shape(nt, R, L, G);
 #define TB_MIXED_TILE(RR)                                                                     \
-  mixed_tile<RR>(lane, wi, tb0 + tbase, nt, L, G, e0, e1, tcx, tcy, tcz, list, src_mask, cbeg, \
-                 cnb, ccen, rel_hi, rel_lo, ss, mt, red, trg)
+  mixed_tile<RR>(lane, wi, tb0 + tbase, nt, L, G, e0, e1, tcx, tcy, tcz, tw, list, src_mask, \
+                 cbeg, cnb, ccen, cmin, cmax, rel_hi, rel_lo, ss, mt, red, trg)
       if (R == 1) TB_MIXED_TILE(1);
       else if (R == 2) TB_MIXED_TILE(2);
       else if (R == 3) TB_MIXED_TILE(3);
@@ -489,7 +528,8 @@ int p2p_mixed(tapas_b200_ctx *ctx) {
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   p2p_mixed_kernel<<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
       ctx->p2p_order.p, nl, ctx->p2p_counter.p, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cbeg.p,
-      ctx->cnb.p, ctx->ccen.p, ctx->rel4.p, ctx->rel_lo.p, ctx->trg.p);
+      ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p, ctx->rel4.p, ctx->rel_lo.p,
+      ctx->trg.p);
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
 }
