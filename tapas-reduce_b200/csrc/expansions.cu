@@ -133,14 +133,11 @@ __global__ void __launch_bounds__(kThreads) m2m_kernel(
   const int ch0 = cchild[c];
   for (int ci = 0; ci < 8; ci++) {
     const int cj = ch0 + ci;
-    double rho, alpha, beta;
-    cart2sph(ccen[3 * c] - ccen[3 * cj], ccen[3 * c + 1] - ccen[3 * cj + 1],
-             ccen[3 * c + 2] - ccen[3 * cj + 2], rho, alpha, beta);
-    const double x = cos(alpha), y = sin(alpha);
-    double sb, cb;
-    sincos(beta, &sb, &cb);
+    if (cnb[cj] == 0) continue;  // an empty child's M is zero
+    const Sph sp = sph_of(ccen[3 * c] - ccen[3 * cj], ccen[3 * c + 1] - ccen[3 * cj + 1],
+                          ccen[3 * c + 2] - ccen[3 * cj + 2]);
     __syncwarp();
-    if (lane < P) multipole_column<P>(lane, rho, x, y, cd{cb, sb}, Y);
+    if (lane < P) multipole_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
     for (int t = lane; t < S::NT; t += 32) {
       double2 v = M[(int64_t)cj * S::NT + t];
       Mj[t] = cd{v.x, v.y};
@@ -207,13 +204,9 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
     const int s = (int)(list[e] & src_mask);
     if (cnb[s] == 0) continue;  // M of an empty cell is exactly zero
     if (use && !use[e]) continue;  // pair evaluated elsewhere (tensor-core classes)
-    double rho, alpha, beta;
-    cart2sph(tx - ccen[3 * s], ty - ccen[3 * s + 1], tz - ccen[3 * s + 2], rho, alpha, beta);
-    const double x = cos(alpha), y = sin(alpha);
-    double sb, cb;
-    sincos(beta, &sb, &cb);
+    const Sph sp = sph_of(tx - ccen[3 * s], ty - ccen[3 * s + 1], tz - ccen[3 * s + 2]);
     __syncwarp();
-    if (lane < P) local_column<P>(lane, rho, x, y, cd{cb, sb}, Y);
+    if (lane < P) local_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
     for (int t = lane; t < S::NT; t += 32) {
       double2 v = M[(int64_t)s * S::NT + t];
       Mj[t] = cd{v.x, v.y};
@@ -263,13 +256,9 @@ __global__ void __launch_bounds__(kThreads) l2l_kernel(
   const int p = cparent[c];
   cd *Y = Ysm[wi];
   cd *Lp = Lsm[wi];
-  double rho, alpha, beta;
-  cart2sph(ccen[3 * c] - ccen[3 * p], ccen[3 * c + 1] - ccen[3 * p + 1],
-           ccen[3 * c + 2] - ccen[3 * p + 2], rho, alpha, beta);
-  const double x = cos(alpha), y = sin(alpha);
-  double sb, cb;
-  sincos(beta, &sb, &cb);
-  if (lane < P) multipole_column<P>(lane, rho, x, y, cd{cb, sb}, Y);
+  const Sph sp = sph_of(ccen[3 * c] - ccen[3 * p], ccen[3 * c + 1] - ccen[3 * p + 1],
+                        ccen[3 * c + 2] - ccen[3 * p + 2]);
+  if (lane < P) multipole_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
   for (int t = lane; t < S::NT; t += 32) {
     double2 v = L[(int64_t)p * S::NT + t];
     Lp[t] = cd{v.x, v.y};
@@ -376,15 +365,15 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
     double *o = trg + 4 * bi;
     // The FP64 near field holds q_i * sum(q_j / r) (the reference's TRG before
     // its `ba /= b.SRC`); the mixed near field is already per unit charge.
-    const double qi = near_has_q ? sq[bi] : 1.0;
-    const double st = sin(theta), ct = cos(theta);
-    const double c0 = st * cp * s0 + ct * cp / r * s1 - sp / r / st * s2;
-    const double c1 = st * sp * s0 + ct * sp / r * s1 + cp / r / st * s2;
-    const double c2 = ct * s0 - st / r * s1;
-    o[0] = o[0] / qi + pot;
-    o[1] = o[1] / qi + c0;
-    o[2] = o[2] / qi + c1;
-    o[3] = o[3] / qi + c2;
+    const double iq = near_has_q ? 1.0 / sq[bi] : 1.0;
+    const double st = y, ct = x;
+    const double c0 = st * cp * s0 + ct * cp * inv_r * s1 - sp * inv_r * inv_y * s2;
+    const double c1 = st * sp * s0 + ct * sp * inv_r * s1 + cp * inv_r * inv_y * s2;
+    const double c2 = ct * s0 - st * inv_r * s1;
+    o[0] = o[0] * iq + pot;
+    o[1] = o[1] * iq + c0;
+    o[2] = o[2] * iq + c1;
+    o[3] = o[3] * iq + c2;
   }
 }
 

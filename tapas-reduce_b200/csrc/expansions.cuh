@@ -35,12 +35,41 @@ struct RecipTable {
 static __constant__ RecipTable kRecip = RecipTable();
 __device__ __forceinline__ double recip(int i) { return kRecip.v[i]; }
 
-// cart2sph (ex/LaplaceSphericalCPU_tapas.h:43-47)
+// cart2sph (ex/LaplaceSphericalCPU_tapas.h:43-47); used per body (P2M, L2P).
 __device__ __forceinline__ void cart2sph(double dx, double dy, double dz, double &r,
                                          double &theta, double &phi) {
   r = sqrt(dx * dx + dy * dy + dz * dz);
   theta = (r == 0) ? 0.0 : acos(dz / r);
   phi = atan2(dy, dx);
+}
+
+// What the translations (M2M, M2L, L2L) need of cart2sph: r, cos(theta),
+// sin(theta) and e^{i phi}, formed directly from the offset instead of through
+// acos, atan2, cos and sin.  r = 0 gives theta = phi = 0 and an offset along
+// the z axis phi = 0, as there.
+struct Sph {
+  double r, x, y;  // r, cos(theta), sin(theta)
+  cd ei;           // e^{i phi}
+};
+__device__ __forceinline__ Sph sph_of(double dx, double dy, double dz) {
+  Sph s;
+  const double rxy2 = dx * dx + dy * dy;
+  s.r = sqrt(rxy2 + dz * dz);
+  s.x = 1.0;
+  s.y = 0.0;
+  s.ei = cd{1.0, 0.0};
+  if (s.r > 0) {
+    const double rxy = sqrt(rxy2), ir = 1.0 / s.r;
+    s.x = dz * ir;
+    s.y = rxy * ir;
+    if (rxy > 0) {
+      const double irxy = 1.0 / rxy;
+      s.ei = cd{dx * irxy, dy * irxy};
+    } else if (dz < 0) {
+      s.y = 1.2246467991473532e-16;  // sin(acos(-1)) in FP64, as the reference gets it
+    }
+  }
+  return s;
 }
 
 // One column m of evalMultipole (:63-99): Ynm for n = m..P-1 written to

@@ -217,12 +217,8 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
   const double Dz = (double)((long long)((key >> 28) & 16383) - kOffBias);
   // offset in units of the target width: D * 2^(min(delta,0) - 1)
   const double u = ldexp(1.0, min(delta, 0) - 1);
-  double rho, alpha, beta;
-  cart2sph(Dx * u, Dy * u, Dz * u, rho, alpha, beta);
-  const double x = cos(alpha), y = sin(alpha);
-  double sb, cb;
-  sincos(beta, &sb, &cb);
-  if (threadIdx.x < P) local_column<P>(threadIdx.x, rho, x, y, cd{cb, sb}, Y);
+  const Sph sp = sph_of(Dx * u, Dy * u, Dz * u);
+  if (threadIdx.x < P) local_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
   __syncthreads();
   float *hi = ops_hi + (size_t)cls * S::MP * S::KP;
   float *lo = ops_lo + (size_t)cls * S::MP * S::KP;
