@@ -5,8 +5,10 @@ Workload (one step = one full FMM evaluation: octree build, upward pass,
 dual-tree traversal with M2L + P2P, downward pass):
   N = 16,000,000 bodies uniform on the unit sphere surface, charges U[-1,1]
   minus their mean, requested relative-L2 potential error 1e-6.  Parameters
-  (P, theta, ncrit) come from the parameter chooser; the result is verified
-  against an FP64 direct sum on 4,000 sampled targets.
+  (P, theta, ncrit) come from the learned chooser: its fastest candidates
+  predicted to meet the tolerance are verified in order against an FP64 direct
+  sum on 4,000 sampled targets (before the timed region) and the first that
+  meets it is timed; the rule table's setting if none does.
 
 Printed JSON line (rank 0):
   value       particles/s of the mixed form, inputs resident in HBM
@@ -321,25 +323,34 @@ def main():
     chooser = import_module("tapas_reduce_b200.chooser")
     if args.P and args.theta and args.ncrit:
         # fixed setting (profiling a given configuration); still verified
-        prm = {"P": args.P, "theta": args.theta, "ncrit": args.ncrit, "precision": "mixed",
-               "source": "fixed by --P/--theta/--ncrit"}
+        tries = [{"P": args.P, "theta": args.theta, "ncrit": args.ncrit, "precision": "mixed",
+                  "source": "fixed by --P/--theta/--ncrit"}]
         ctx.partition(*dev, ncrit=args.ncrit)  # the direct-sum check reads the bodies
     else:
+        # the learned chooser's candidates, fastest predicted first; each is
+        # verified against the direct sum and the first that meets tol is used
         feats = chooser.system_features(ctx, *dev)
-        prm = chooser.choose_params(n, args.tol, "mixed", features=feats, ctx=ctx)
+        tries = chooser.candidates(ctx, feats, n, args.tol, "mixed", k=3)
     d_check = ctx.direct(tg)
-    try:
-        ctx.evaluate(*dev, P=prm["P"], ncrit=prm["ncrit"], theta=prm["theta"],
-                     precision=tb.MIXED, out=out_dev)
-        e_check = orc.rel_l2(out_dev.cpu().numpy()[tg], d_check)[0]
-    except tb.TapasError as err:  # e.g. a setting too large for device memory
-        prm["error"] = str(err)
-        e_check = float("inf")
-    prm["verified_rel_l2_pot"] = e_check
-    if e_check > args.tol:
-        missed = dict(prm)
+    prm, tried = None, []
+    for cand in tries:
+        cand = dict(cand)
+        try:
+            ctx.evaluate(*dev, P=cand["P"], ncrit=cand["ncrit"], theta=cand["theta"],
+                         precision=tb.MIXED, out=out_dev)
+            e_check = orc.rel_l2(out_dev.cpu().numpy()[tg], d_check)[0]
+        except tb.TapasError as err:  # e.g. a setting too large for device memory
+            cand["error"] = str(err)
+            e_check = float("inf")
+        cand["verified_rel_l2_pot"] = e_check
+        if e_check <= args.tol:
+            prm = cand
+            break
+        tried.append(cand)
+    if prm is None:  # no candidate verified: the rule table's setting
         prm = choose(tb, n, args.tol, "mixed")
-        prm["after_miss_of"] = missed
+    if tried:
+        prm["missed_before"] = tried
     P, theta, ncrit = prm["P"], prm["theta"], prm["ncrit"]
     torch.cuda.synchronize()
 

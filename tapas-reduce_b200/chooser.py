@@ -121,10 +121,33 @@ class LearnedChooser:
         else:  # nothing predicted to meet it: the most accurate candidate
             idx = int(np.argmin(pred[:, 0]))
             src = "learned-best-effort"
+        return self._setting(g, pred, idx, src)
+
+    @staticmethod
+    def _setting(g, pred, idx, src):
         P, th, nc, f64 = g[idx]
         return {"P": int(P), "theta": float(th), "ncrit": int(nc),
                 "precision": "fp64" if f64 else "mixed", "source": src,
                 "pred_log10_err": float(pred[idx, 0]), "pred_log10_ms": float(pred[idx, 1])}
+
+    def ranked(self, features: np.ndarray, tol: float, precisions=(0, 1), k: int = 3) -> list:
+        """Settings to try in order, for a caller that verifies each one: up to
+        k - 1 of the fastest candidates predicted to meet `tol` without the
+        safety margin, then the margin-safe choice of `choose`."""
+        g = candidate_grid()
+        g = g[np.isin(g[:, 3], precisions)]
+        f = np.array(features, dtype=np.float64)
+        f[0] = min(max(f[0], 4.0), 6.0)
+        pred = self.predict(encode(f, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
+        safe = self.choose(features, tol, precisions)
+        out = []
+        ok = np.flatnonzero(pred[:, 0] <= np.log10(tol))
+        for idx in ok[np.argsort(pred[ok, 1], kind="stable")]:
+            if len(out) >= k - 1 or pred[idx, 1] >= safe["pred_log10_ms"]:
+                break
+            out.append(self._setting(g, pred, idx, "learned-unmargined"))
+        out.append(safe)
+        return out
 
 
 _cache = {}
@@ -163,22 +186,43 @@ def choose_params(n: int, tol: float, precision: str = "mixed", features=None,
     return dict(FIXED, source="fixed")
 
 
-def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=None):
-    """Chosen setting -> evaluation -> FP64 direct-sum check on `targets` ->
-    fixed fallback on a miss.  Returns (results, info)."""
+def candidates(ctx, features, n: int, tol: float, precision: str = "auto", k: int = 3) -> list:
+    """Settings to verify in order: the learned chooser's ranked candidates
+    when a model is present, else the rule table's setting."""
+    lc = learned_chooser(ctx) if (ctx is not None and features is not None) else None
+    if lc is not None:
+        precs = {"mixed": (0,), "fp64": (1,), "auto": (0, 1)}[precision]
+        return lc.ranked(features, tol, precs, k)
+    return [choose_params(n, tol, precision)]
+
+
+def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=None, k=3):
+    """Chosen settings -> evaluation -> FP64 direct-sum check on `targets`:
+    the learned chooser's candidates are tried in order (at most k) and the
+    first that meets `tol` is kept; the fixed setting is the fallback when
+    none does.  Returns (results, info)."""
     from importlib import import_module
     rel_l2 = import_module("tapas_reduce_b200.verify").rel_l2
     if params is None:
         if features is None:
             features = system_features(ctx, x, y, z, q)
-        params = choose_params(len(x), tol, "auto", features=features, ctx=ctx)
-    prec = tb.FP64 if params["precision"] == "fp64" else tb.MIXED
-    res = ctx.evaluate(x, y, z, q, P=params["P"], ncrit=params["ncrit"], theta=params["theta"],
-                       precision=prec)
-    d = ctx.direct(targets)
-    err = rel_l2(res[targets], d)
+        tries = candidates(ctx, features, len(x), tol, "auto", k)
+    else:
+        tries = [params]
+    d = None
+    tried = []
+    for params in tries:
+        prec = tb.FP64 if params["precision"] == "fp64" else tb.MIXED
+        res = ctx.evaluate(x, y, z, q, P=params["P"], ncrit=params["ncrit"],
+                           theta=params["theta"], precision=prec)
+        if d is None:
+            d = ctx.direct(targets)
+        err = rel_l2(res[targets], d)
+        tried.append({"params": params, "rel_l2_pot": err[0]})
+        if err[0] <= tol:
+            break
     info = {"params": params, "rel_l2_pot": err[0], "rel_l2_acc": err[1],
-            "met": err[0] <= tol, "fallback": False}
+            "met": err[0] <= tol, "fallback": False, "tried": tried}
     if not info["met"]:
         res = ctx.evaluate(x, y, z, q, P=FIXED["P"], ncrit=FIXED["ncrit"], theta=FIXED["theta"],
                            precision=tb.FP64)

@@ -183,6 +183,7 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->front_a.release();
   ctx->front_b.release();
   ctx->counters.release();
+  ctx->cell_r.release();
   ctx->M.release();
   ctx->L.release();
   mixed_release(ctx);

@@ -155,6 +155,7 @@ struct tapas_b200_ctx {
   tb::DBuf<uint64_t> ckey;
   tb::DBuf<int32_t> cbeg, cnb, cparent, cchild, cleaf, clevel;
   tb::DBuf<double> cmin, cmax, ccen;    // 3 doubles per cell (x,y,z interleaved)
+  tb::DBuf<double> cell_r;              // traversal: per-cell MAC radius for the current theta
   tb::DBuf<int32_t> flag, flag_scan;    // per-level scratch
   tb::DBuf<int32_t> leaf_list;          // indices of non-empty leaves
   int64_t n_nonempty_leaves = 0;

@@ -29,17 +29,25 @@ constexpr int kBlock = 256;
 
 struct CellView {
   const int32_t *leaf, *nb, *child;
-  const double *mn, *mx, *cen;
+  const double *cen;
+  const double *R;  // per cell: (max width / 2 * 1.00001) / theta
 };
 
-__device__ __forceinline__ double cell_R(const CellView &c, int i, double theta) {
-  double R = 0;
+// R of every cell for this theta, with the reference's operations in its
+// order (max over the widths, halve, * 1.00001, / theta), computed once per
+// traversal instead of twice per visited pair.
+__global__ void cell_radii(int64_t ncells, const double *__restrict__ mn,
+                           const double *__restrict__ mx, double theta, double *__restrict__ R) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double w = 0;
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    double w = __dsub_rn(c.mx[3 * i + d], c.mn[3 * i + d]);
-    R = (R < w) ? w : R;  // std::max(R, w)
+    for (int d = 0; d < 3; d++) {
+      const double wd = __dsub_rn(mx[3 * i + d], mn[3 * i + d]);
+      w = (w < wd) ? wd : w;  // std::max(R, w)
+    }
+    R[i] = __ddiv_rn(__dmul_rn(w / 2, 1.00001), theta);
   }
-  return __ddiv_rn(__dmul_rn(R / 2, 1.00001), theta);
 }
 
 // Warp-aggregated reservation of `cnt` slots per lane in a global counter.
@@ -92,7 +100,7 @@ __global__ void __launch_bounds__(kBlock) dtt_step(CellView c, double theta,
       double R2 = __dadd_rn(0.0, __dmul_rn(dx, dx));
       R2 = __dadd_rn(R2, __dmul_rn(dy, dy));
       R2 = __dadd_rn(R2, __dmul_rn(dz, dz));
-      const double Ri = cell_R(c, t, theta), Rj = cell_R(c, s, theta);
+      const double Ri = c.R[t], Rj = c.R[s];
       const double RR = __dadd_rn(Ri, Rj);
       const bool lt = c.leaf[t] != 0, ls = c.leaf[s] != 0;
       if (R2 > __dmul_rn(RR, RR)) {
@@ -195,7 +203,11 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
   ctx->theta = theta;
   ctx->have_lists = false;
   const int64_t C = ctx->ncells;
-  CellView cv{ctx->cleaf.p, ctx->cnb.p, ctx->cchild.p, ctx->cmin.p, ctx->cmax.p, ctx->ccen.p};
+  TB_CUDA(ctx, ctx->cell_r.ensure(C + 1, s));
+  cell_radii<<<grid_for(C, kBlock), kBlock, 0, s>>>(C, ctx->cmin.p, ctx->cmax.p, theta,
+                                                    ctx->cell_r.p);
+  TB_LAUNCH_CHECK(ctx);
+  CellView cv{ctx->cleaf.p, ctx->cnb.p, ctx->cchild.p, ctx->ccen.p, ctx->cell_r.p};
   TB_CUDA(ctx, ctx->counters.ensure(8, s));
   TB_CUDA(ctx, ctx->pinned.ensure(256));
   unsigned long long *hc = reinterpret_cast<unsigned long long *>(ctx->pinned.p);
