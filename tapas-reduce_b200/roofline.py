@@ -16,6 +16,16 @@ figure exists for them.
 from __future__ import annotations
 
 
+# DRAM bytes of one p2p_mixed_kernel launch per body, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum = 47.4 MB + 11.5 MB on a 1M-body
+# unit-sphere-surface set, P=10, theta=0.25, ncrit=128).  The kernel's DRAM
+# traffic is its body arrays read and results written (its source re-reads hit
+# L2), so a launch's traffic is this figure times the bodies.
+P2P_MIXED_DRAM_BYTES_PER_BODY = 58.9
+# Same capture, m2l_tc_kernel<10>: 531 MB + 8.7 MB for 2.67M translations.
+M2L_TC_DRAM_BYTES_PER_TRANSLATION = 202.0
+
+
 def m2l_flops_per_translation(P: int) -> int:
     return 8 * sum((j + 1) * (P - j) ** 2 for j in range(P))
 
@@ -49,7 +59,10 @@ def dominant(phases: dict, lists: dict, tree: dict, P: int, peaks: dict, peak_sr
         peak = float(peaks.get("bf16_tflops", 1590.0)) / 2
         ach = fl / (ms * 1e-3) / 1e12
         out.update(bound="tensor", achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
-                   peak_source=f"TF32 dense = bf16 {peak_src} / 2", traffic=None,
+                   peak_source=f"TF32 dense = bf16 {peak_src} / 2",
+                   traffic=M2L_TC_DRAM_BYTES_PER_TRANSLATION * ntc,
+                   traffic_source="ncu DRAM bytes per translation of a 1M-body capture, "
+                                  "scaled by the translations",
                    executed_mma_tflops=executed / (ms * 1e-3) / 1e12,
                    work=f"{ntc} translations x {m2l_flops_per_translation(P)} flop "
                         f"(algorithmic); MMA executes 3 x 2 x 128 x {mp} x {kp} per tile")
@@ -61,8 +74,11 @@ def dominant(phases: dict, lists: dict, tree: dict, P: int, peaks: dict, peak_sr
         kind = "fp32" if precision == "mixed" else "fp64"
         peak = nominal_tflops(kind, smx)
         ach = fl / (ms * 1e-3) / 1e12
+        traffic = P2P_MIXED_DRAM_BYTES_PER_BODY * n if precision == "mixed" else None
         out.update(bound=kind, achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
-                   peak_source=f"nominal {kind} at {smx:.0f} MHz", traffic=None,
+                   peak_source=f"nominal {kind} at {smx:.0f} MHz", traffic=traffic,
+                   traffic_source=("ncu DRAM bytes per body of a 1M-body capture, scaled by "
+                                   "the bodies" if traffic else None),
                    work=f"{lists['n_p2p_interactions']} interactions x 20 flop")
     elif name == "m2l":
         fl = float(m2l_flops_per_translation(P)) * lists["n_m2l"]
