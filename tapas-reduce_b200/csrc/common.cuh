@@ -185,6 +185,11 @@ struct tapas_b200_ctx {
   tb::DBuf<uint64_t> p2p_wkey, p2p_wkey_alt;  // P2P work order: keys
   tb::DBuf<uint32_t> p2p_order, p2p_order_alt;  // target leaves by decreasing work
   tb::DBuf<int> p2p_counter;            // P2P work-queue head
+  tb::DBuf<int4> p2p_items;             // P2P work items (leaf, list range, partial rows)
+  tb::DBuf<int32_t> p2p_kcnt, p2p_koff, p2p_psz, p2p_poff;  // per leaf: pieces, partial rows
+  tb::DBuf<double> p2p_part;            // partial sums of pieces of split leaves
+  int64_t p2p_nitems = 0;
+  bool p2p_split = false;
   tb::TcState tc;                       // mixed: tensor-core M2L work state
   const uint8_t *m2l_use = nullptr;     // FP64 M2L: evaluate only pairs with use[e] != 0
   int64_t tc_classes = 0, tc_tiles = 0, tc_segments = 0, n_m2l_tc = 0;

@@ -29,6 +29,12 @@ void mixed_release(tapas_b200_ctx *ctx) {
   ctx->p2p_order.release();
   ctx->p2p_order_alt.release();
   ctx->p2p_counter.release();
+  ctx->p2p_items.release();
+  ctx->p2p_kcnt.release();
+  ctx->p2p_koff.release();
+  ctx->p2p_psz.release();
+  ctx->p2p_poff.release();
+  ctx->p2p_part.release();
   ctx->tc.release();
 }
 

@@ -41,29 +41,116 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kThreads = 32 * kWarps;
 constexpr int kStage = 32;   // source bodies staged per warp at a time (one per lane)
-constexpr int kMaxR = 4;     // targets per lane: leaves up to 128 bodies per pass
-// mixed kernel: 4-warp CTAs, 3 per SM (up to 170 registers a thread, 12 warps per SM)
+constexpr int kMaxR = 3;     // FP64: targets per lane, leaves up to 96 bodies per pass
+// mixed kernel: 4-warp CTAs, 4 per SM (<= 128 registers, 16 warps per SM), up to
+// 3 targets per lane (leaves of more than 96 bodies take two passes)
 constexpr int kMixedWarps = 4;
 constexpr int kMixedThreads = 32 * kMixedWarps;
-constexpr int kMixedBlocks = 3;
 
 // ---------------------------------------------------------------------------
-// work order: target leaves by decreasing nt * sum(ns)
+// work items: a target leaf with its source list, or a piece of a long list
 // ---------------------------------------------------------------------------
-__global__ void leaf_work_keys(const int32_t *__restrict__ leaves, int64_t nleaves,
-                               const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
-                               uint64_t src_mask, const int32_t *__restrict__ cnb,
-                               uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+// A target leaf whose source list holds more than kSplitSources bodies (a big
+// leaf beside a dense region, e.g. the core of a Plummer sphere) is split into
+// consecutive list ranges of about that many sources, so no single warp
+// carries it alone.  A piece writes its partial sums to its own rows of a
+// scratch array; split_reduce adds a leaf's pieces in order, so the result
+// does not depend on which warp finished first.
+constexpr int64_t kSplitSources = 32768;
+
+struct WorkItem {
+  int32_t leaf, e0, e1;  // target leaf (cell index) and its list range [e0, e1)
+  int32_t pbase;         // -1: writes trg directly; else first row of its partials
+};
+
+// per non-empty leaf w: pieces k (>= 1) and partial rows (k * nt when split)
+__global__ void leaf_pieces(const int32_t *__restrict__ leaves, int64_t nleaves,
+                            const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
+                            uint64_t src_mask, const int32_t *__restrict__ cnb,
+                            int32_t *__restrict__ kcnt, int32_t *__restrict__ psz) {
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nleaves;
        w += (int64_t)gridDim.x * blockDim.x) {
     const int c = leaves[w];
-    uint64_t ns = 0;
-    for (int e = off[c]; e < off[c + 1]; e++) ns += (uint64_t)cnb[(int)(list[e] & src_mask)];
-    uint64_t work = ns * (uint64_t)cnb[c];
-    if (work > 0xFFFFFFFFull) work = 0xFFFFFFFFull;
-    keys[w] = 0xFFFFFFFFull - work;  // ascending sort -> decreasing work
-    vals[w] = (uint32_t)c;
+    int64_t ns = 0;
+    for (int e = off[c]; e < off[c + 1]; e++) ns += cnb[(int)(list[e] & src_mask)];
+    const int64_t k = ns > kSplitSources ? (ns + kSplitSources - 1) / kSplitSources : 1;
+    kcnt[w] = (int32_t)k;
+    psz[w] = k > 1 ? (int32_t)(k * cnb[c]) : 0;
   }
+}
+
+// Items of leaf w at koff[w]..: cut its list greedily where the sources
+// reach kSplitSources (at most k pieces; unused slots become empty pieces with
+// zeroed partials).  Work key = nt * sources of the piece, for the queue.
+__global__ void emit_items(const int32_t *__restrict__ leaves, int64_t nleaves,
+                           const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
+                           uint64_t src_mask, const int32_t *__restrict__ cnb,
+                           const int32_t *__restrict__ kcnt, const int32_t *__restrict__ koff,
+                           const int32_t *__restrict__ poff, WorkItem *__restrict__ items,
+                           uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                           double *__restrict__ part) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nleaves;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int c = leaves[w];
+    const int e0 = off[c], e1 = off[c + 1], k = kcnt[w], nt = cnb[c];
+    const int base = koff[w];
+    int j = 0, ea = e0;
+    int64_t acc = 0;
+    for (int e = e0; e < e1; e++) {
+      acc += cnb[(int)(list[e] & src_mask)];
+      if ((k > 1 && acc >= kSplitSources && j < k - 1) || e == e1 - 1) {
+        uint64_t work = (uint64_t)acc * (uint64_t)nt;
+        if (work > 0xFFFFFFFFull) work = 0xFFFFFFFFull;
+        items[base + j] = WorkItem{c, ea, e + 1, k > 1 ? poff[w] + j * nt : -1};
+        keys[base + j] = 0xFFFFFFFFull - work;  // ascending sort -> decreasing work
+        vals[base + j] = (uint32_t)(base + j);
+        j++;
+        ea = e + 1;
+        acc = 0;
+      }
+    }
+    if (e1 == e0) {  // no list: one empty item still writes the leaf's zero sums
+      items[base] = WorkItem{c, e0, e0, -1};
+      keys[base] = 0xFFFFFFFFull;
+      vals[base] = (uint32_t)base;
+      j = 1;
+    }
+    for (; j < k; j++) {  // unused pieces: empty, zero partials
+      items[base + j] = WorkItem{c, e1, e1, poff[w] + j * nt};
+      keys[base + j] = 0xFFFFFFFFull;
+      vals[base + j] = (uint32_t)(base + j);
+      for (int t = 0; t < 4 * nt; t++) part[4 * ((int64_t)poff[w] + (int64_t)j * nt) + t] = 0.0;
+    }
+  }
+}
+
+// trg rows of split leaves = sum of their pieces' partial rows, in piece order
+__global__ void split_reduce(const int32_t *__restrict__ leaves, int64_t nleaves,
+                             const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
+                             const int32_t *__restrict__ kcnt, const int32_t *__restrict__ poff,
+                             const double *__restrict__ part, double *__restrict__ trg) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nleaves;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int k = kcnt[w];
+    if (k <= 1) continue;
+    const int c = leaves[w], nt = cnb[c], b0 = cbeg[c];
+    for (int t = 0; t < nt; t++) {
+      double4 acc = make_double4(0, 0, 0, 0);
+      for (int j = 0; j < k; j++) {
+        const double4 v =
+            reinterpret_cast<const double4 *>(part)[(int64_t)poff[w] + (int64_t)j * nt + t];
+        acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+      }
+      reinterpret_cast<double4 *>(trg)[b0 + t] = acc;
+    }
+  }
+}
+
+// Where a work item's sums go: trg rows of its leaf, or its partial rows.
+__device__ __forceinline__ double4 *item_out(const WorkItem &it, int tb0, double *trg,
+                                             double *part) {
+  return it.pbase < 0 ? reinterpret_cast<double4 *>(trg) + tb0
+                      : reinterpret_cast<double4 *>(part) + it.pbase;
 }
 
 __device__ __forceinline__ int next_leaf(int *counter, int lane) {
@@ -84,7 +171,7 @@ __device__ __forceinline__ void fp64_tile(int lane, int wi, int tb0, int nt, int
                                           const double *__restrict__ sy,
                                           const double *__restrict__ sz,
                                           const double *__restrict__ sq, double4 (*src)[32],
-                                          double *__restrict__ trg) {
+                                          double4 *__restrict__ out) {
   double xi[kR], yi[kR], zi[kR], qi[kR], pot[kR], ax[kR], ay[kR], az[kR];
 #pragma unroll
   for (int r = 0; r < kR; r++) {
@@ -129,35 +216,37 @@ __device__ __forceinline__ void fp64_tile(int lane, int wi, int tb0, int nt, int
 #pragma unroll
   for (int r = 0; r < kR; r++) {
     const int i = lane + 32 * r;
-    if (i < nt)
-      reinterpret_cast<double4 *>(trg)[tb0 + i] = make_double4(pot[r], ax[r], ay[r], az[r]);
+    if (i < nt) out[i] = make_double4(pot[r], ax[r], ay[r], az[r]);
   }
 }
 
-__global__ void __launch_bounds__(kThreads) p2p_fp64_kernel(
-    const uint32_t *__restrict__ order, int64_t nleaves, int *__restrict__ counter,
-    const int32_t *__restrict__ off, const uint64_t *__restrict__ list, uint64_t src_mask,
+// 3 CTAs of 8 warps per SM (<= 85 registers)
+__global__ void __launch_bounds__(kThreads, 3) p2p_fp64_kernel(
+    const uint32_t *__restrict__ order, int64_t nitems, int *__restrict__ counter,
+    const WorkItem *__restrict__ items, const uint64_t *__restrict__ list, uint64_t src_mask,
     const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
     const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
-    const double *__restrict__ sq, double *__restrict__ trg) {
+    const double *__restrict__ sq, double *__restrict__ trg, double *__restrict__ part) {
   __shared__ double4 src[kWarps][32];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   for (;;) {
     const int w = next_leaf(counter, lane);
-    if (w >= nleaves) break;
-    const int c = (int)order[w];
+    if (w >= nitems) break;
+    const WorkItem it = items[order[w]];
+    if (it.pbase >= 0 && it.e0 == it.e1) continue;  // unused piece of a split list
+    const int c = it.leaf;
     const int tb0 = cbeg[c], nt_all = cnb[c];
-    const int e0 = off[c], e1 = off[c + 1];
+    const int e0 = it.e0, e1 = it.e1;
+    double4 *out = item_out(it, tb0, trg, part);
     for (int tbase = 0; tbase < nt_all; tbase += 32 * kMaxR) {
       const int nt = min(nt_all - tbase, 32 * kMaxR);
       const int R = (nt + 31) / 32;
 #define TB_FP64_TILE(RR)                                                                    \
   fp64_tile<RR>(lane, wi, tb0 + tbase, nt, e0, e1, list, src_mask, cbeg, cnb, sx, sy, sz, sq, \
-                src, trg)
+                src, out + tbase)
       if (R == 1) TB_FP64_TILE(1);
       else if (R == 2) TB_FP64_TILE(2);
-      else if (R == 3) TB_FP64_TILE(3);
-      else TB_FP64_TILE(4);
+      else TB_FP64_TILE(3);
 #undef TB_FP64_TILE
     }
   }
@@ -203,14 +292,15 @@ __device__ __forceinline__ float two_sum(float a, float b, float &e) {
 
 // Shape of a mixed tile of nt targets: kR targets per lane, L = ceil(nt/kR)
 // lanes per group, G = 32/L groups that split the sources.  Time per source
-// ~ kR / G, so pick the kR in 1..kMaxR that minimises it (ties: the larger
-// kR, fewer shared loads per interaction).  nt <= 32 * kMaxR.
+// ~ kR / G, so pick the kR in 1..kMaxRm that minimises it (ties: the larger
+// kR, fewer shared loads per interaction).  nt <= 32 * kMaxRm.
+template <int kMaxRm>
 __device__ __forceinline__ void mixed_shape(int nt, int &R, int &L, int &G) {
-  R = kMaxR;
-  L = (nt + kMaxR - 1) / kMaxR;
+  R = kMaxRm;
+  L = (nt + kMaxRm - 1) / kMaxRm;
   G = 32 / L;
 #pragma unroll
-  for (int r = kMaxR - 1; r >= 1; r--) {
+  for (int r = kMaxRm - 1; r >= 1; r--) {
     const int l = (nt + r - 1) / r;
     if (l > 32) break;
     const int g = 32 / l;
@@ -262,7 +352,7 @@ __device__ __forceinline__ void mixed_tile(
     const double *__restrict__ ccen, const double *__restrict__ cmin,
     const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
     const float4 *__restrict__ rel_lo, SrcRec (*ss)[kStage],
-    LeafMeta (*mt)[32], double4 (*red)[32], double *__restrict__ trg) {
+    LeafMeta (*mt)[32], double4 (*red)[32], double4 *__restrict__ out) {
   const int g = lane / L, tl = lane - g * L;
   const bool active = g < G;
   const int gs = active ? g : kStage;  // idle lanes skip the source loop
@@ -422,62 +512,93 @@ __device__ __forceinline__ void mixed_tile(
       }
     }
     const int t = tl + L * r;
-    if (active && g == 0 && t < nt) reinterpret_cast<double4 *>(trg)[tb0 + t] = v;
+    if (active && g == 0 && t < nt) out[t] = v;
   }
 }
 
-__global__ void __launch_bounds__(kMixedThreads, kMixedBlocks) p2p_mixed_kernel(
-    const uint32_t *__restrict__ order, int64_t nleaves, int *__restrict__ counter,
-    const int32_t *__restrict__ off, const uint64_t *__restrict__ list, uint64_t src_mask,
+template <int kMaxRm, int kBlocks>
+__global__ void __launch_bounds__(kMixedThreads, kBlocks) p2p_mixed_kernel(
+    const uint32_t *__restrict__ order, int64_t nitems, int *__restrict__ counter,
+    const WorkItem *__restrict__ items, const uint64_t *__restrict__ list, uint64_t src_mask,
     const int32_t *__restrict__ cbeg, const int32_t *__restrict__ cnb,
     const double *__restrict__ ccen, const double *__restrict__ cmin,
     const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
-    const float4 *__restrict__ rel_lo, double *__restrict__ trg) {
+    const float4 *__restrict__ rel_lo, double *__restrict__ trg, double *__restrict__ part) {
   __shared__ SrcRec ss[kMixedWarps][kStage];
   __shared__ LeafMeta mt[kMixedWarps][32];
   __shared__ double4 red[kMixedWarps][32];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   for (;;) {
     const int w = next_leaf(counter, lane);
-    if (w >= nleaves) break;
-    const int c = (int)order[w];
+    if (w >= nitems) break;
+    const WorkItem it = items[order[w]];
+    if (it.pbase >= 0 && it.e0 == it.e1) continue;  // unused piece of a split list
+    const int c = it.leaf;
     const int tb0 = cbeg[c], nt_all = cnb[c];
-    const int e0 = off[c], e1 = off[c + 1];
+    const int e0 = it.e0, e1 = it.e1;
+    double4 *out = item_out(it, tb0, trg, part);
     const double tcx = ccen[3 * c], tcy = ccen[3 * c + 1], tcz = ccen[3 * c + 2];
     const double tw = cmax[3 * c] - cmin[3 * c];
-    for (int tbase = 0; tbase < nt_all; tbase += 32 * kMaxR) {
-      const int nt = min(nt_all - tbase, 32 * kMaxR);
+    for (int tbase = 0; tbase < nt_all; tbase += 32 * kMaxRm) {
+      const int nt = min(nt_all - tbase, 32 * kMaxRm);
       int R, L, G;
-      mixed_shape(nt, R, L, G);
+      mixed_shape<kMaxRm>(nt, R, L, G);
 #define TB_MIXED_TILE(RR)                                                                     \
   mixed_tile<RR>(lane, wi, tb0 + tbase, nt, L, G, e0, e1, tcx, tcy, tcz, tw, list, src_mask, \
-                 cbeg, cnb, ccen, cmin, cmax, rel_hi, rel_lo, ss, mt, red, trg)
+                 cbeg, cnb, ccen, cmin, cmax, rel_hi, rel_lo, ss, mt, red, out + tbase)
       if (R == 1) TB_MIXED_TILE(1);
       else if (R == 2) TB_MIXED_TILE(2);
-      else if (R == 3) TB_MIXED_TILE(3);
-      else TB_MIXED_TILE(4);
+      else if (kMaxRm == 3 || R == 3) TB_MIXED_TILE(3);
+      else TB_MIXED_TILE(kMaxRm);
 #undef TB_MIXED_TILE
     }
   }
 }
 
-// Builds ctx->p2p_order (target leaves by decreasing work) for the current lists.
-int p2p_order(tapas_b200_ctx *ctx) {
+// Builds the P2P work items of the current lists (ctx->p2p_items) and their
+// queue order (ctx->p2p_order: items by decreasing work).
+int p2p_items(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
   const int64_t nl = ctx->n_nonempty_leaves;
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
-  TB_CUDA(ctx, ctx->p2p_wkey.ensure(nl + 1, s));
-  TB_CUDA(ctx, ctx->p2p_wkey_alt.ensure(nl + 1, s));
-  TB_CUDA(ctx, ctx->p2p_order.ensure(nl + 1, s));
-  TB_CUDA(ctx, ctx->p2p_order_alt.ensure(nl + 1, s));
+  TB_CUDA(ctx, ctx->p2p_kcnt.ensure(nl + 1, s));
+  TB_CUDA(ctx, ctx->p2p_koff.ensure(nl + 1, s));
+  TB_CUDA(ctx, ctx->p2p_psz.ensure(nl + 1, s));
+  TB_CUDA(ctx, ctx->p2p_poff.ensure(nl + 1, s));
+  leaf_pieces<<<grid_for(nl, 256), 256, 0, s>>>(ctx->leaf_list.p, nl, ctx->p2p_off.p, ctx->p2p.p,
+                                                 mask, ctx->cnb.p, ctx->p2p_kcnt.p,
+                                                 ctx->p2p_psz.p);
+  TB_LAUNCH_CHECK(ctx);
+  TB_TRY(scan_exclusive(ctx, ctx->p2p_kcnt.p, ctx->p2p_koff.p, nl, ctx->p2p_koff.p + nl));
+  TB_TRY(scan_exclusive(ctx, ctx->p2p_psz.p, ctx->p2p_poff.p, nl, ctx->p2p_poff.p + nl));
+  TB_CUDA(ctx, ctx->pinned.ensure(256));
+  int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, ctx->p2p_koff.p + nl, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaMemcpyAsync(h + 1, ctx->p2p_poff.p + nl, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  const int64_t ni = h[0], npart = h[1];
+  if (ni < nl || npart < 0) {
+    set_error(ctx, "p2p: work item count overflow");
+    return TAPAS_B200_ERR_CAPACITY;
+  }
+  ctx->p2p_nitems = ni;
+  ctx->p2p_split = npart > 0;
+  TB_CUDA(ctx, ctx->p2p_items.ensure((size_t)ni * sizeof(WorkItem) / sizeof(int4) + 1, s));
+  TB_CUDA(ctx, ctx->p2p_part.ensure(4 * (size_t)npart + 4, s));
+  TB_CUDA(ctx, ctx->p2p_wkey.ensure(ni + 1, s));
+  TB_CUDA(ctx, ctx->p2p_wkey_alt.ensure(ni + 1, s));
+  TB_CUDA(ctx, ctx->p2p_order.ensure(ni + 1, s));
+  TB_CUDA(ctx, ctx->p2p_order_alt.ensure(ni + 1, s));
   TB_CUDA(ctx, ctx->p2p_counter.ensure(4, s));
-  leaf_work_keys<<<grid_for(nl, 256), 256, 0, s>>>(ctx->leaf_list.p, nl, ctx->p2p_off.p,
-                                                    ctx->p2p.p, mask, ctx->cnb.p,
-                                                    ctx->p2p_wkey.p, ctx->p2p_order.p);
+  emit_items<<<grid_for(nl, 256), 256, 0, s>>>(
+      ctx->leaf_list.p, nl, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cnb.p, ctx->p2p_kcnt.p,
+      ctx->p2p_koff.p, ctx->p2p_poff.p, reinterpret_cast<WorkItem *>(ctx->p2p_items.p),
+      ctx->p2p_wkey.p, ctx->p2p_order.p, ctx->p2p_part.p);
   TB_LAUNCH_CHECK(ctx);
   uint64_t *k = ctx->p2p_wkey.p, *ka = ctx->p2p_wkey_alt.p;
   uint32_t *v = ctx->p2p_order.p, *va = ctx->p2p_order_alt.p;
-  TB_TRY(radix_sort(ctx, k, ka, v, va, nl, 0, 32));
+  TB_TRY(radix_sort(ctx, k, ka, v, va, ni, 0, 32));
   if (v != ctx->p2p_order.p) {
     std::swap(ctx->p2p_order.p, ctx->p2p_order_alt.p);
     std::swap(ctx->p2p_order.cap, ctx->p2p_order_alt.cap);
@@ -490,11 +611,22 @@ int p2p_order(tapas_b200_ctx *ctx) {
   return TAPAS_B200_OK;
 }
 
-int p2p_grid(tapas_b200_ctx *ctx, int warps_per_block) {
-  // persistent: enough warps to fill the GPU, never more than the leaves
+// Adds the pieces of split leaves into trg (after a P2P kernel).
+int p2p_finish(tapas_b200_ctx *ctx) {
+  if (!ctx->p2p_split) return TAPAS_B200_OK;
   const int64_t nl = ctx->n_nonempty_leaves;
+  split_reduce<<<grid_for(nl, 256), 256, 0, ctx->stream>>>(
+      ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->p2p_kcnt.p, ctx->p2p_poff.p,
+      ctx->p2p_part.p, ctx->trg.p);
+  TB_LAUNCH_CHECK(ctx);
+  return TAPAS_B200_OK;
+}
+
+int p2p_grid(tapas_b200_ctx *ctx, int warps_per_block) {
+  // persistent: enough warps to fill the GPU, never more than the work items
+  const int64_t ni = ctx->p2p_nitems;
   int64_t g = (int64_t)ctx->num_sms * (64 / warps_per_block);
-  const int64_t need = (nl + warps_per_block - 1) / warps_per_block;
+  const int64_t need = (ni + warps_per_block - 1) / warps_per_block;
   return (int)std::max<int64_t>(1, std::min(g, need));
 }
 
@@ -504,13 +636,14 @@ int p2p_fp64(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
   const int64_t nl = ctx->n_nonempty_leaves;
   if (nl == 0) return TAPAS_B200_OK;
-  TB_TRY(p2p_order(ctx));
+  TB_TRY(p2p_items(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   p2p_fp64_kernel<<<p2p_grid(ctx, kWarps), kThreads, 0, s>>>(
-      ctx->p2p_order.p, nl, ctx->p2p_counter.p, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cbeg.p,
-      ctx->cnb.p, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->trg.p);
+      ctx->p2p_order.p, ctx->p2p_nitems, ctx->p2p_counter.p,
+      reinterpret_cast<const WorkItem *>(ctx->p2p_items.p), ctx->p2p.p, mask, ctx->cbeg.p,
+      ctx->cnb.p, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->trg.p, ctx->p2p_part.p);
   TB_LAUNCH_CHECK(ctx);
-  return TAPAS_B200_OK;
+  return p2p_finish(ctx);
 }
 
 int p2p_mixed(tapas_b200_ctx *ctx) {
@@ -524,14 +657,17 @@ int p2p_mixed(tapas_b200_ctx *ctx) {
                                                       ctx->sy.p, ctx->sz.p, ctx->sq.p,
                                                       ctx->rel4.p, ctx->rel_lo.p);
   TB_LAUNCH_CHECK(ctx);
-  TB_TRY(p2p_order(ctx));
+  TB_TRY(p2p_items(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
-  p2p_mixed_kernel<<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
-      ctx->p2p_order.p, nl, ctx->p2p_counter.p, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cbeg.p,
+  // up to 3 targets per lane at 16 warps per SM: measured faster than 4 targets at
+  // 12 warps in most sphere, cube and Plummer sets of 1M-16M bodies, ncrit 16-128
+  p2p_mixed_kernel<3, 4><<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
+      ctx->p2p_order.p, ctx->p2p_nitems, ctx->p2p_counter.p,
+      reinterpret_cast<const WorkItem *>(ctx->p2p_items.p), ctx->p2p.p, mask, ctx->cbeg.p,
       ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p, ctx->rel4.p, ctx->rel_lo.p,
-      ctx->trg.p);
+      ctx->trg.p, ctx->p2p_part.p);
   TB_LAUNCH_CHECK(ctx);
-  return TAPAS_B200_OK;
+  return p2p_finish(ctx);
 }
 
 }  // namespace tb

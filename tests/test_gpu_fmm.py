@@ -168,10 +168,14 @@ def test_against_reference_goldens(path, tb, ctx):
         assert _rel(L[order][ne], g["L"][ne]) < FP64_RTOL
 
 
-def test_mixed_close_to_fp64(tb, ctx, oracle_mod):
-    x, y, z, q = tb.datasets.make("plummer", 40000, 21)
-    r64 = ctx.evaluate(x, y, z, q, P=10, ncrit=64, theta=0.4, precision=tb.FP64)
-    rmx = ctx.evaluate(x, y, z, q, P=10, ncrit=64, theta=0.4, precision=tb.MIXED)
+@pytest.mark.parametrize("dist,ncrit", [("plummer", 64), ("plummer", 16),
+                                        ("sphere_surface", 128), ("uniform_cube", 128)])
+def test_mixed_close_to_fp64(dist, ncrit, tb, ctx, oracle_mod):
+    """Mixed near field and tensor-core M2L against the FP64 form: small
+    leaves (4-target P2P tiles) and full leaves (3-target tiles at 16 warps)."""
+    x, y, z, q = tb.datasets.make(dist, 40000, 21)
+    r64 = ctx.evaluate(x, y, z, q, P=10, ncrit=ncrit, theta=0.4, precision=tb.FP64)
+    rmx = ctx.evaluate(x, y, z, q, P=10, ncrit=ncrit, theta=0.4, precision=tb.MIXED)
     ep, ea = oracle_mod.rel_l2(rmx, r64)
     assert ep < 2e-6 and ea < 2e-6
     tg = tb.datasets.sample_targets(len(x), 500)
@@ -295,3 +299,27 @@ def test_device_pointers(tb, ctx):
     torch.cuda.synchronize()
     ctx.evaluate(dx, dy, dz, dq, P=6, ncrit=32, theta=0.4, out=out)
     assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_long_source_lists_are_split(tb, ctx):
+    """A Plummer set has leaves whose near-field lists hold far more than the
+    32,768 source bodies one P2P work item takes; those lists are cut into
+    pieces whose partial sums are added in piece order, so the FP64 form stays
+    bit-reproducible and both forms keep their accuracy."""
+    x, y, z, q = tb.datasets.make("plummer", 200000, 31)
+    ctx.partition(x, y, z, q, ncrit=64)
+    ctx.build_lists(0.3)
+    c = ctx.cells()
+    _, (pt, ps) = ctx.lists()
+    per_target = np.bincount(pt, weights=c["nb"][ps].astype(np.float64), minlength=len(c["nb"]))
+    assert per_target.max() > 4 * 32768  # the case is exercised
+    a = ctx.evaluate(x, y, z, q, P=8, ncrit=64, theta=0.3, precision=tb.FP64)
+    b = ctx.evaluate(x, y, z, q, P=8, ncrit=64, theta=0.3, precision=tb.FP64)
+    assert np.array_equal(a, b)
+    tg = tb.datasets.sample_targets(len(x), 400, seed=5)
+    d = ctx.direct(tg)
+    num = np.linalg.norm(a[tg] - d, axis=0)
+    den = np.linalg.norm(d, axis=0)
+    assert num[0] / den[0] < 1e-5 and np.linalg.norm(num[1:]) / np.linalg.norm(den[1:]) < 1e-4
+    m = ctx.evaluate(x, y, z, q, P=8, ncrit=64, theta=0.3, precision=tb.MIXED)
+    assert np.linalg.norm(m[:, 0] - a[:, 0]) / np.linalg.norm(a[:, 0]) < 2e-6
