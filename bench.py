@@ -19,6 +19,9 @@ Printed JSON line (rank 0):
   roofline    the dominant kernel of the step against its bound
   cpu_baseline  the reference's own CPU implementation (oracle/_ref, built from
               the reference sources) on a bounded sample of the same workload
+  configs     the other measured configurations: 100k cube against the
+              reference's own output, 1M Plummer (FP64 vs mixed), 4M-body
+              Barnes-Hut (skipped with --no-configs)
 
 Multi-GPU: replicas only (the path is one tree per GPU); each rank evaluates its
 own seeded body set, value = all ranks' bodies / max-over-ranks time.
@@ -291,6 +294,9 @@ def main():
     ap.add_argument("--ncrit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (100k cube vs the reference, 1M "
+                         "Plummer, 4M Barnes-Hut)")
     ap.add_argument("--ref-sample", type=int, default=REF_SAMPLE_N,
                     help="bodies per reference CPU step (--impl reference)")
     ap.add_argument("--ref-threads", type=int, default=0,
@@ -437,6 +443,17 @@ def main():
         v, kind, secs = cpu_reference_run(tb, orc)
         cpu = cpu_baseline_obj(v, kind, secs)
 
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = {}
+        for key, fn in (("cube_1e5", config_cube_100k), ("plummer_1e6", config_plummer_1m),
+                        ("barnes_hut_plummer_4e6", config_bh_4m)):
+            try:
+                configs[key] = fn(tb, orc, ctx, torch, stream)
+            except Exception as err:  # reported, never fatal to the headline line
+                configs[key] = {"error": str(err)}
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
@@ -455,12 +472,132 @@ def main():
                 "work": {"n_m2l": li["n_m2l"], "n_p2p_interactions": li["n_p2p_interactions"],
                          "n_cells": ti["n_cells"], "max_depth": ti["max_depth"]},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "configs": configs,
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------
+# the other measured configurations (rank 0, one GPU)
+# ---------------------------------------------------------------------------
+def _timed(torch, stream, fn, reps=3):
+    """Median CUDA-event time (ms) of fn() on `stream` after one warm-up call."""
+    fn()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def _rel(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def config_cube_100k(tb, orc, ctx, torch, stream):
+    """100,000 bodies uniform in [-1,1]^3, charges U[0,1] summing to 1, P=10,
+    theta=0.4, ncrit=64: both forms against the FP64 direct sum on 1,000
+    targets and against the reference's own FP64 output on the same bodies."""
+    n = 100_000
+    x, y, z, q = tb.datasets.make("uniform_cube", n, 101)
+    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
+    out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    tg = tb.datasets.sample_targets(n, 1000, seed=7)
+    res = {"workload": "uniform cube N=1e5 q=U[0,1]/sum P=10 theta=0.4 ncrit=64"}
+    ref = None
+    if orc.reference_available(10):
+        R = orc.run_reference(x, y, z, q, P=10, ncrit=64, theta=0.4)
+        b = R["bodies"]
+        ref = np.empty((n, 4))
+        ref[b["ibody"]] = b["trg"]
+        t = R["times"]
+        res["reference_cpu_1core_ms"] = 1e3 * (t["tree"] + t["upward"] + t["traverse"] + t["downward"])
+    for prec, name in ((tb.FP64, "fp64"), (tb.MIXED, "mixed")):
+        ms = _timed(torch, stream, lambda: ctx.evaluate(*dev, P=10, ncrit=64, theta=0.4,
+                                                         precision=prec, out=out))
+        r = out.cpu().numpy()
+        d = ctx.direct(tg)
+        e = {"ms": ms, "rel_l2_pot_vs_direct": _rel(r[tg, 0], d[:, 0]),
+             "rel_l2_acc_vs_direct": _rel(r[tg, 1:], d[:, 1:])}
+        if ref is not None:
+            e["rel_l2_pot_vs_reference"] = _rel(r[:, 0], ref[:, 0])
+            e["rel_l2_acc_vs_reference"] = _rel(r[:, 1:], ref[:, 1:])
+        res[name] = e
+    return res
+
+
+def config_plummer_1m(tb, orc, ctx, torch, stream):
+    """1M Plummer bodies (scale radius 1, r < 100), charges 1/N, P=10,
+    theta=0.4, ncrit=64: plain FP64 against the mixed form, errors against the
+    FP64 direct sum on 2,000 targets."""
+    n = 1_000_000
+    x, y, z, q = tb.datasets.make("plummer", n, 102)
+    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
+    out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    tg = tb.datasets.sample_targets(n, 2000, seed=8)
+    res = {"workload": "Plummer N=1e6 q=1/N P=10 theta=0.4 ncrit=64"}
+    for prec, name in ((tb.FP64, "fp64"), (tb.MIXED, "mixed")):
+        ms = _timed(torch, stream, lambda: ctx.evaluate(*dev, P=10, ncrit=64, theta=0.4,
+                                                         precision=prec, out=out))
+        r = out.cpu().numpy()
+        d = ctx.direct(tg)
+        res[name] = {"ms": ms, "particles_per_s": n / (ms * 1e-3),
+                     "rel_l2_pot_vs_direct": _rel(r[tg, 0], d[:, 0]),
+                     "rel_l2_acc_vs_direct": _rel(r[tg, 1:], d[:, 1:])}
+    res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+    return res
+
+
+def config_bh_4m(tb, orc, ctx, torch, stream):
+    """Barnes-Hut: 4M Plummer bodies, monopoles, theta=0.5, ncrit=32, softening
+    1e-6: the FP32 walk (FP64 moments) and the FP64 walk; force error against
+    a softened FP64 direct sum on 2,000 targets (self term included, as in the
+    sample); interactions/s of the walk and tree-build bytes/s."""
+    n = 4_000_000
+    x, y, z, m = tb.datasets.make("plummer", n, 103)
+    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, m)]
+    out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    tg = tb.datasets.sample_targets(n, 2000, seed=9)
+    eps2 = 1e-6
+    # softened FP64 direct sum for the sampled targets, on the GPU in chunks
+    X = torch.stack(dev[:3], 1)
+    M = dev[3]
+    d = torch.zeros((len(tg), 4), dtype=torch.float64, device="cuda")
+    tt = X[torch.from_numpy(tg).cuda()]
+    chunk = 1 << 14  # 2,000 x 16,384 x 3 doubles = 0.8 GB per temporary
+    for c0 in range(0, n, chunk):
+        dx = X[None, c0:c0 + chunk, :] - tt[:, None, :]
+        ir = torch.rsqrt((dx * dx).sum(-1) + eps2)
+        mi = M[None, c0:c0 + chunk] * ir
+        d[:, :3] += (dx * (mi * ir * ir)[..., None]).sum(1)
+        d[:, 3] += mi.sum(1)
+        del dx, ir, mi
+    d = d.cpu().numpy()
+    res = {"workload": "Barnes-Hut Plummer N=4e6 theta=0.5 ncrit=32 eps2=1e-6"}
+    for prec, name in ((tb.MIXED, "fp32_walk"), (tb.FP64, "fp64_walk")):
+        ctx.set_profiling(True)
+        ms = _timed(torch, stream, lambda: ctx.bh_evaluate(*dev, ncrit=32, theta=0.5, eps2=eps2,
+                                                            precision=prec, out=out))
+        t = ctx.timings()
+        ctx.set_profiling(False)
+        na, nd = ctx.bh_counts()
+        r = out.cpu().numpy()
+        build_ms = t["bbox_keys"] + t["sort"] + t["tree"]
+        res[name] = {"ms": ms, "interactions_per_s": (na + nd) / (ms * 1e-3),
+                     "approx": na, "direct": nd,
+                     "tree_build_ms": build_ms,
+                     "tree_build_gbs": 316.0 * n / (build_ms * 1e-3) / 1e9,
+                     "rel_l2_force_vs_direct": _rel(r[tg, :3], d[:, :3]),
+                     "rel_l2_pot_vs_direct": _rel(r[tg, 3], d[:, 3])}
+    return res
 
 
 def _peaks():
