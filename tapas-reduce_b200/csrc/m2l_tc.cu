@@ -43,8 +43,6 @@ namespace {
 
 constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor cores
 constexpr int kNTile = 128;        // pairs per tile (MMA N)
-constexpr uint64_t kKeyEmpty = 0xFFFFFFFFFFFFull;  // source has no bodies: no work
-constexpr uint64_t kKeyRare = 0xFFFFFFFFFFFEull;   // offset outside the key range: FP64
 constexpr int kOffBias = 8192;
 
 template <int P>
@@ -74,37 +72,96 @@ struct TcShape {
 // ---------------------------------------------------------------------------
 // classification
 // ---------------------------------------------------------------------------
+// Offset class of an M2L pair: the level difference delta = depth_t - depth_s
+// and D = (c_t - c_s) / (w_min / 2), an integer vector; false when a cell is
+// empty (no work) or the offset is not a whole number of half-widths or too
+// large for the operator's key (those pairs stay on the FP64 kernel).
+__device__ __forceinline__ int pair_class(int t, int s, const int32_t *__restrict__ cnb,
+                                          const int32_t *__restrict__ clevel,
+                                          const double *__restrict__ cmin,
+                                          const double *__restrict__ cmax,
+                                          const double *__restrict__ ccen, int &delta,
+                                          long long D[3]) {
+  if (cnb[s] == 0 || cnb[t] == 0) return 0;  // empty
+  delta = clevel[t] - clevel[s];
+  const double wt = cmax[3 * t] - cmin[3 * t], ws = cmax[3 * s] - cmin[3 * s];
+  const double half = 0.5 * fmin(wt, ws);
+  bool ok = delta > -32 && delta < 32;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double r = (ccen[3 * t + d] - ccen[3 * s + d]) / half;
+    D[d] = llrint(r);
+    ok = ok && fabs(r - (double)D[d]) < 1e-3 && D[d] > -kOffBias && D[d] < kOffBias;
+  }
+  return ok ? 2 : 1;  // 2: a class; 1: FP64
+}
+
+// Largest |D| component and |delta| over the classed pairs (for the key width).
+__global__ void class_ranges(int64_t n, const uint64_t *__restrict__ list, int shift,
+                             const int32_t *__restrict__ cnb, const int32_t *__restrict__ clevel,
+                             const double *__restrict__ cmin, const double *__restrict__ cmax,
+                             const double *__restrict__ ccen, int *__restrict__ ranges) {
+  const uint64_t mask = (1ull << shift) - 1;
+  int md = 0, ml = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = list[e];
+    int delta;
+    long long D[3];
+    if (pair_class((int)(v >> shift), (int)(v & mask), cnb, clevel, cmin, cmax, ccen, delta,
+                   D) == 2) {
+      md = max(md, (int)max(llabs(D[0]), max(llabs(D[1]), llabs(D[2]))));
+      ml = max(ml, abs(delta));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    md = max(md, __shfl_xor_sync(0xffffffffu, md, o));
+    ml = max(ml, __shfl_xor_sync(0xffffffffu, ml, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(ranges, md);
+    atomicMax(ranges + 1, ml);
+  }
+}
+
+// Sort key of a class, as narrow as the lists allow: delta + bd in the top db
+// bits, then D_z, D_y, D_x + bo in cb bits each; the two largest codes of the
+// (db + 3 cb + 1)-bit range mark empty and FP64 pairs.
+struct KeyPack {
+  int cb, db, bo, bd, bits;
+  __host__ __device__ uint64_t empty() const { return (1ull << bits) - 1; }
+  __host__ __device__ uint64_t rare() const { return (1ull << bits) - 2; }
+  __device__ uint64_t pack(int delta, const long long D[3]) const {
+    return ((uint64_t)(delta + bd) << (3 * cb)) | ((uint64_t)(D[2] + bo) << (2 * cb)) |
+           ((uint64_t)(D[1] + bo) << cb) | (uint64_t)(D[0] + bo);
+  }
+  // the operator builder's fixed 48-bit form of a packed class
+  __device__ uint64_t wide(uint64_t k) const {
+    const uint64_t m = (1ull << cb) - 1;
+    const long long dx = (long long)(k & m) - bo, dy = (long long)((k >> cb) & m) - bo,
+                    dz = (long long)((k >> (2 * cb)) & m) - bo;
+    const int delta = (int)(k >> (3 * cb)) - bd;
+    return ((uint64_t)(delta + 32) << 42) | ((uint64_t)(dz + kOffBias) << 28) |
+           ((uint64_t)(dy + kOffBias) << 14) | (uint64_t)(dx + kOffBias);
+  }
+};
+
 __global__ void classify_pairs(int64_t n, const uint64_t *__restrict__ list, int shift,
                                const int32_t *__restrict__ cnb,
                                const int32_t *__restrict__ clevel,
                                const double *__restrict__ cmin, const double *__restrict__ cmax,
-                               const double *__restrict__ ccen, uint64_t *__restrict__ keys,
-                               uint32_t *__restrict__ vals) {
+                               const double *__restrict__ ccen, KeyPack kp,
+                               uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
   const uint64_t mask = (1ull << shift) - 1;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
        e += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t v = list[e];
-    const int t = (int)(v >> shift), s = (int)(v & mask);
-    uint64_t key;
-    if (cnb[s] == 0 || cnb[t] == 0) {
-      key = kKeyEmpty;
-    } else {
-      const int delta = clevel[t] - clevel[s];
-      const double wt = cmax[3 * t] - cmin[3 * t], ws = cmax[3 * s] - cmin[3 * s];
-      const double half = 0.5 * fmin(wt, ws);
-      bool ok = delta > -32 && delta < 32;
-      long long D[3];
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const double r = (ccen[3 * t + d] - ccen[3 * s + d]) / half;
-        D[d] = llrint(r);
-        ok = ok && fabs(r - (double)D[d]) < 1e-3 && D[d] > -kOffBias && D[d] < kOffBias;
-      }
-      key = ok ? ((uint64_t)(delta + 32) << 42) | ((uint64_t)(D[2] + kOffBias) << 28) |
-                     ((uint64_t)(D[1] + kOffBias) << 14) | (uint64_t)(D[0] + kOffBias)
-               : kKeyRare;
-    }
-    keys[e] = key;
+    int delta = 0;
+    long long D[3];
+    const int kind =
+        pair_class((int)(v >> shift), (int)(v & mask), cnb, clevel, cmin, cmax, ccen, delta, D);
+    keys[e] = kind == 0 ? kp.empty() : (kind == 1 ? kp.rare() : kp.pack(delta, D));
     vals[e] = (uint32_t)e;
   }
 }
@@ -126,13 +183,13 @@ __global__ void segment_starts(const int32_t *__restrict__ flag, const int32_t *
 
 // per class: is it a tensor-core class?
 __global__ void class_tc_flags(const int32_t *__restrict__ seg_start, int64_t nseg, int64_t n,
-                               const uint64_t *__restrict__ keys, int64_t min_count,
+                               const uint64_t *__restrict__ keys, KeyPack kp, int64_t min_count,
                                int32_t *__restrict__ tcflag, int32_t *__restrict__ ntiles) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
        c += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
     const uint64_t k = keys[b];
-    const bool tc = (k != kKeyEmpty) && (k != kKeyRare) && (e - b) >= min_count;
+    const bool tc = (k != kp.empty()) && (k != kp.rare()) && (e - b) >= min_count;
     tcflag[c] = tc ? 1 : 0;
     ntiles[c] = tc ? (int32_t)((e - b + kNTile - 1) / kNTile) : 0;
   }
@@ -142,14 +199,14 @@ __global__ void class_tc_flags(const int32_t *__restrict__ seg_start, int64_t ns
 __global__ void mark_fp64_pairs(const int32_t *__restrict__ seg_scan_incl_flag,
                                 const int32_t *__restrict__ scan, const int32_t *__restrict__ flag,
                                 const int32_t *__restrict__ tcflag,
-                                const uint64_t *__restrict__ keys,
+                                const uint64_t *__restrict__ keys, KeyPack kp,
                                 const uint32_t *__restrict__ vals, int64_t n,
                                 uint8_t *__restrict__ use64) {
   (void)seg_scan_incl_flag;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int cls = scan[i] + flag[i] - 1;  // inclusive scan - 1
-    const bool empty = keys[i] == kKeyEmpty;
+    const bool empty = keys[i] == kp.empty();
     use64[vals[i]] = (!empty && !tcflag[cls]) ? 1 : 0;
   }
 }
@@ -164,14 +221,15 @@ struct TileItem {
 __global__ void build_tiles(const int32_t *__restrict__ seg_start, int64_t nseg, int64_t n,
                             const int32_t *__restrict__ tcflag, const int32_t *__restrict__ tcid,
                             const int32_t *__restrict__ tile_off,
-                            const uint64_t *__restrict__ keys, uint64_t *__restrict__ tc_keys,
-                            TileItem *__restrict__ items, int *__restrict__ tc_pairs) {
+                            const uint64_t *__restrict__ keys, KeyPack kp,
+                            uint64_t *__restrict__ tc_keys, TileItem *__restrict__ items,
+                            int *__restrict__ tc_pairs) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
        c += (int64_t)gridDim.x * blockDim.x) {
     if (!tcflag[c]) continue;
     const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
     const int id = tcid[c];
-    tc_keys[id] = keys[b];
+    tc_keys[id] = kp.wide(keys[b]);
     atomicAdd(tc_pairs, (int)(e - b));
     int64_t o = tile_off[c];
     for (int64_t p = b; p < e; p += kNTile, o++) {
@@ -338,14 +396,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait (about 2 s of SM clock); false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > 4000000000LL) return false;
-  }
-  return true;
-}
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
@@ -741,14 +791,38 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_CUDA(ctx, T.vals_alt.ensure(n + 1, s));
   TB_CUDA(ctx, T.use64.ensure(n + 1, s));
   if (n == 0) return TAPAS_B200_OK;
+  // key width from the lists' largest offsets
+  TB_CUDA(ctx, T.err.ensure(4, s));
+  TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
+  class_ranges<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+      n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
+      ctx->ccen.p, T.err.p + 2);
+  TB_LAUNCH_CHECK(ctx);
+  TB_CUDA(ctx, ctx->pinned.ensure(256));
+  int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p + 2, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  KeyPack kp;
+  {
+    auto bits_for = [](int64_t range) {  // bits holding 0..range
+      int b = 1;
+      while (((int64_t)1 << b) <= range) b++;
+      return b;
+    };
+    kp.bo = h[0];
+    kp.bd = h[1];
+    kp.cb = bits_for(2 * (int64_t)h[0]);
+    kp.db = bits_for(2 * (int64_t)h[1]);
+    kp.bits = kp.db + 3 * kp.cb + 1;
+  }
   classify_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
       n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
-      ctx->ccen.p, T.keys.p, T.vals.p);
+      ctx->ccen.p, kp, T.keys.p, T.vals.p);
   TB_LAUNCH_CHECK(ctx);
   {
     uint64_t *k = T.keys.p, *ka = T.keys_alt.p;
     uint32_t *v = T.vals.p, *va = T.vals_alt.p;
-    TB_TRY(radix_sort(ctx, k, ka, v, va, n, 0, 48));
+    TB_TRY(radix_sort(ctx, k, ka, v, va, n, 0, kp.bits));
     if (k != T.keys.p) { std::swap(T.keys.p, T.keys_alt.p); std::swap(T.keys.cap, T.keys_alt.cap); }
     if (v != T.vals.p) { std::swap(T.vals.p, T.vals_alt.p); std::swap(T.vals.cap, T.vals_alt.cap); }
   }
@@ -758,8 +832,6 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   segment_flags<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.keys.p, n, T.flag.p);
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(scan_exclusive(ctx, T.flag.p, T.scan.p, n, T.scan.p + n));
-  TB_CUDA(ctx, ctx->pinned.ensure(256));
-  int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
   TB_CUDA(ctx, cudaMemcpyAsync(h, T.scan.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TB_CUDA(ctx, cudaStreamSynchronize(s));
   const int64_t nseg = h[0];
@@ -789,13 +861,13 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
       min_count = std::max<int64_t>(kTcMin, cnt[max_classes - 1] + 1);
     }
   }
-  class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p, min_count,
-                                                      T.tcflag.p, T.ntiles.p);
+  class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p, kp,
+                                                      min_count, T.tcflag.p, T.ntiles.p);
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(scan_exclusive(ctx, T.tcflag.p, T.tcid.p, nseg, T.tcid.p + nseg));
   TB_TRY(scan_exclusive(ctx, T.ntiles.p, T.tile_off.p, nseg, T.tile_off.p + nseg));
   mark_fp64_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
-      nullptr, T.scan.p, T.flag.p, T.tcflag.p, T.keys.p, T.vals.p, n, T.use64.p);
+      nullptr, T.scan.p, T.flag.p, T.tcflag.p, T.keys.p, kp, T.vals.p, n, T.use64.p);
   TB_LAUNCH_CHECK(ctx);
   TB_CUDA(ctx, cudaMemcpyAsync(h, T.tcid.p + nseg, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TB_CUDA(ctx, cudaMemcpyAsync(h + 1, T.tile_off.p + nseg, sizeof(int32_t),
@@ -811,7 +883,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_CUDA(ctx, T.err.ensure(4, s));
   TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
   build_tiles<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.tcflag.p, T.tcid.p,
-                                                   T.tile_off.p, T.keys.p, T.tc_keys.p,
+                                                   T.tile_off.p, T.keys.p, kp, T.tc_keys.p,
                                                    reinterpret_cast<TileItem *>(T.items.p),
                                                    T.err.p + 1);
   TB_LAUNCH_CHECK(ctx);
