@@ -77,6 +77,7 @@ typedef struct {
   int64_t n_m2l_tc;            /* translations evaluated on the tensor cores       */
   int64_t tc_classes;          /* offset classes run as GEMMs                      */
   int64_t tc_tiles;            /* 128-translation GEMM tiles                       */
+  int64_t pairs_visited;       /* (target, source) pairs the traversal classified  */
 } tapas_b200_list_stats;
 
 /* Phase timings of the last calls, milliseconds, measured with CUDA events on

@@ -48,7 +48,8 @@ class ListStats(ctypes.Structure):
     _fields_ = [("n_m2l", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
                 ("n_p2p_interactions", ctypes.c_uint64),
                 ("traverse_iterations", ctypes.c_int32), ("n_m2l_tc", ctypes.c_int64),
-                ("tc_classes", ctypes.c_int64), ("tc_tiles", ctypes.c_int64)]
+                ("tc_classes", ctypes.c_int64), ("tc_tiles", ctypes.c_int64),
+                ("pairs_visited", ctypes.c_int64)]
 
 
 _TIMING_FIELDS = ("upload", "bbox_keys", "sort", "tree", "upward", "p2m", "m2m", "traverse",

@@ -177,13 +177,15 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
     b->release();
   for (auto *b : {&ctx->idx, &ctx->idx_alt, &ctx->sort_hist}) b->release();
   for (auto *b : {&ctx->scan_tmp, &ctx->cbeg, &ctx->cnb, &ctx->cparent, &ctx->cchild, &ctx->cleaf,
-                  &ctx->clevel, &ctx->flag, &ctx->flag_scan, &ctx->leaf_list, &ctx->m2l_off,
-                  &ctx->p2p_off, &ctx->m2l_tlist, &ctx->p2p_tlist})
+                  &ctx->clevel, &ctx->flag, &ctx->flag_scan, &ctx->leaf_list, &ctx->list_cnt,
+                  &ctx->m2l_off, &ctx->p2p_off, &ctx->m2l_tlist, &ctx->p2p_tlist})
     b->release();
   ctx->front_a.release();
   ctx->front_b.release();
   ctx->counters.release();
-  ctx->cell_r.release();
+  ctx->trav_geo.release();
+  ctx->trav_meta.release();
+  ctx->list_src.release();
   ctx->M.release();
   ctx->L.release();
   mixed_release(ctx);
@@ -409,6 +411,7 @@ int tapas_b200_list_info(tapas_b200_ctx *ctx, tapas_b200_list_stats *out) {
   out->n_m2l_tc = ctx->n_m2l_tc;
   out->tc_classes = ctx->tc_classes;
   out->tc_tiles = ctx->tc_tiles;
+  out->pairs_visited = ctx->trav_pairs;
   return TAPAS_B200_OK;
 }
 

@@ -155,7 +155,8 @@ struct tapas_b200_ctx {
   tb::DBuf<uint64_t> ckey;
   tb::DBuf<int32_t> cbeg, cnb, cparent, cchild, cleaf, clevel;
   tb::DBuf<double> cmin, cmax, ccen;    // 3 doubles per cell (x,y,z interleaved)
-  tb::DBuf<double> cell_r;              // traversal: per-cell MAC radius for the current theta
+  tb::DBuf<double4> trav_geo;          // traversal: per cell {centre, MAC radius for this theta}
+  tb::DBuf<int2> trav_meta;            // traversal: per cell {nb, first child or -1 for a leaf}
   tb::DBuf<int32_t> flag, flag_scan;    // per-level scratch
   tb::DBuf<int32_t> leaf_list;          // indices of non-empty leaves
   int64_t n_nonempty_leaves = 0;
@@ -166,10 +167,13 @@ struct tapas_b200_ctx {
   tb::DBuf<int2> front_a, front_b;      // (target, source) pairs
   tb::DBuf<uint64_t> m2l, p2p;          // (target << 32 | source)
   tb::DBuf<uint64_t> list_alt;
+  tb::DBuf<int32_t> list_cnt;           // list ordering: per-target counts, cursors, long segments
+  tb::DBuf<uint32_t> list_src;          // list ordering: sources grouped by target
   tb::DBuf<unsigned long long> counters; // [next, m2l, p2p, p2p_interactions, overflow]
   int64_t n_m2l = 0, n_p2p = 0;
   uint64_t n_p2p_int = 0;
   int trav_iters = 0;
+  int64_t trav_pairs = 0;  // (target, source) pairs the traversal classified
   int list_shift = 1;                   // packed list key = target << shift | source
   bool reference_lists = false;         // keep pairs with empty cells, as the reference visits them
   tb::DBuf<int32_t> m2l_off, p2p_off;   // CSR by target cell, ncells+1

@@ -27,17 +27,22 @@ namespace {
 
 constexpr int kBlock = 256;
 
-struct CellView {
-  const int32_t *leaf, *nb, *child;
-  const double *cen;
-  const double *R;  // per cell: (max width / 2 * 1.00001) / theta
+// What one visit reads of a cell, packed so a visit touches two sectors per
+// cell: geometry {cx, cy, cz, R} with R = (max width / 2 * 1.00001) / theta,
+// and {nb, first child or -1 for a leaf}.
+struct TravCells {
+  const double4 *geo;
+  const int2 *meta;
 };
 
-// R of every cell for this theta, with the reference's operations in its
-// order (max over the widths, halve, * 1.00001, / theta), computed once per
-// traversal instead of twice per visited pair.
-__global__ void cell_radii(int64_t ncells, const double *__restrict__ mn,
-                           const double *__restrict__ mx, double theta, double *__restrict__ R) {
+// The traversal's cell records for this theta, with the reference's
+// operations in its order for R (max over the widths, halve, * 1.00001,
+// / theta), computed once per traversal instead of twice per visited pair.
+__global__ void trav_cells(int64_t ncells, const double *__restrict__ mn,
+                           const double *__restrict__ mx, const double *__restrict__ cen,
+                           const int32_t *__restrict__ nb, const int32_t *__restrict__ leaf,
+                           const int32_t *__restrict__ child, double theta,
+                           double4 *__restrict__ geo, int2 *__restrict__ meta) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells;
        i += (int64_t)gridDim.x * blockDim.x) {
     double w = 0;
@@ -46,115 +51,132 @@ __global__ void cell_radii(int64_t ncells, const double *__restrict__ mn,
       const double wd = __dsub_rn(mx[3 * i + d], mn[3 * i + d]);
       w = (w < wd) ? wd : w;  // std::max(R, w)
     }
-    R[i] = __ddiv_rn(__dmul_rn(w / 2, 1.00001), theta);
+    const double R = __ddiv_rn(__dmul_rn(w / 2, 1.00001), theta);
+    geo[i] = make_double4(cen[3 * i + 0], cen[3 * i + 1], cen[3 * i + 2], R);
+    meta[i] = make_int2(nb[i], leaf[i] ? -1 : child[i]);
   }
 }
 
-// Warp-aggregated reservation of `cnt` slots per lane in a global counter.
-__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *ctr, unsigned cnt,
-                                                           unsigned &my_off) {
-  const unsigned lane = threadIdx.x & 31;
-  // Inclusive prefix of cnt across the warp.
-  unsigned incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= (unsigned)o) incl += t;
-  }
-  unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-  unsigned long long base = 0;
-  if (lane == 31 && total) base = atomicAdd(ctr, (unsigned long long)total);
-  base = __shfl_sync(0xffffffffu, base, 31);
-  my_off = incl - cnt;
-  return base;
-}
+// Per-thread output counts packed in one word for the block scan: M2L pairs
+// in bits 0-9, P2P pairs in bits 10-19, new frontier pairs in bits 20-31
+// (at most 256, 256 and 8 * 256 per block).
+constexpr int kWarpsPerBlock = kBlock / 32;
+static_assert(kBlock <= 256, "packed per-block counts hold at most 256 threads");
 
 // counters: [0] next frontier size, [1] m2l size, [2] p2p size,
 //           [3] p2p body-pair interactions, [4] overflow flag
-__global__ void __launch_bounds__(kBlock) dtt_step(CellView c, double theta,
-                                                   const int2 *__restrict__ front, int64_t nfront,
-                                                   int2 *__restrict__ next, int64_t next_cap,
-                                                   uint64_t *__restrict__ m2l, int64_t m2l_cap,
-                                                   uint64_t *__restrict__ p2p, int64_t p2p_cap,
+// Slots in the three outputs are reserved once per block (one atomic per
+// counter per block), the block's threads taking consecutive slots.
+__global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__restrict__ front,
+                                                   int64_t nfront, int2 *__restrict__ next,
+                                                   int64_t next_cap, uint64_t *__restrict__ m2l,
+                                                   int64_t m2l_cap, uint64_t *__restrict__ p2p,
+                                                   int64_t p2p_cap,
                                                    unsigned long long *__restrict__ counters,
                                                    int prune_empty) {
+  __shared__ uint32_t wsum[kWarpsPerBlock];
+  __shared__ unsigned long long wint[kWarpsPerBlock];
+  __shared__ unsigned long long bbase[3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nfront;
        base += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = base + threadIdx.x;
     int kind = 0;  // 0 none, 1 m2l, 2 p2p, 3 split target, 4 split source
-    int t = 0, s = 0;
+    int t = 0, s = 0, split_child = 0;
     unsigned long long inter = 0;
-    bool live = i < nfront;
-    if (live) {
-      int2 pr = front[i];
+    if (i < nfront) {
+      const int2 pr = front[i];
       t = pr.x;
       s = pr.y;
+      const int2 mt = c.meta[t], ms = c.meta[s];
       // An empty cell (and so all of its descendants) contributes nothing as a
       // source and receives nothing used later as a target.
-      if (prune_empty && (c.nb[t] == 0 || c.nb[s] == 0)) live = false;
-    }
-    if (live) {
-      const double dx = __dsub_rn(c.cen[3 * t + 0], c.cen[3 * s + 0]);
-      const double dy = __dsub_rn(c.cen[3 * t + 1], c.cen[3 * s + 1]);
-      const double dz = __dsub_rn(c.cen[3 * t + 2], c.cen[3 * s + 2]);
-      double R2 = __dadd_rn(0.0, __dmul_rn(dx, dx));
-      R2 = __dadd_rn(R2, __dmul_rn(dy, dy));
-      R2 = __dadd_rn(R2, __dmul_rn(dz, dz));
-      const double Ri = c.R[t], Rj = c.R[s];
-      const double RR = __dadd_rn(Ri, Rj);
-      const bool lt = c.leaf[t] != 0, ls = c.leaf[s] != 0;
-      if (R2 > __dmul_rn(RR, RR)) {
-        kind = 1;
-      } else if (lt && ls) {
-        const int nt = c.nb[t], ns = c.nb[s];
-        if (nt > 0 && ns > 0) {
-          kind = 2;
-          inter = (unsigned long long)nt * (unsigned long long)ns;
+      if (!prune_empty || (mt.x != 0 && ms.x != 0)) {
+        const double4 gt = c.geo[t], gs = c.geo[s];
+        const double dx = __dsub_rn(gt.x, gs.x);
+        const double dy = __dsub_rn(gt.y, gs.y);
+        const double dz = __dsub_rn(gt.z, gs.z);
+        double R2 = __dadd_rn(0.0, __dmul_rn(dx, dx));
+        R2 = __dadd_rn(R2, __dmul_rn(dy, dy));
+        R2 = __dadd_rn(R2, __dmul_rn(dz, dz));
+        const double Ri = gt.w, Rj = gs.w;
+        const double RR = __dadd_rn(Ri, Rj);
+        const bool lt = mt.y < 0, ls = ms.y < 0;
+        if (R2 > __dmul_rn(RR, RR)) {
+          kind = 1;
+        } else if (lt && ls) {
+          if (mt.x > 0 && ms.x > 0) {
+            kind = 2;
+            inter = (unsigned long long)mt.x * (unsigned long long)ms.x;
+          }
+        } else if (ls) {
+          kind = 3;
+        } else if (lt) {
+          kind = 4;
+        } else {
+          kind = (Ri >= Rj) ? 3 : 4;
         }
-      } else if (ls) {
-        kind = 3;
-      } else if (lt) {
-        kind = 4;
-      } else {
-        kind = (Ri >= Rj) ? 3 : 4;
+        split_child = kind == 3 ? mt.y : ms.y;
       }
     }
-    unsigned off;
-    // M2L
-    unsigned long long b1 = warp_reserve(counters + 1, kind == 1, off);
+    const uint32_t mine = (kind == 1 ? 1u : 0u) | (kind == 2 ? 1u << 10 : 0u) |
+                          (kind >= 3 ? 8u << 20 : 0u);
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    unsigned long long w = inter;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if (lane == 31) wsum[warp] = incl;
+    if (lane == 0) wint[warp] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      unsigned long long tot = 0;
+#pragma unroll
+      for (int k = 0; k < kWarpsPerBlock; k++) {
+        const uint32_t v = wsum[k];
+        wsum[k] = run;
+        run += v;
+        tot += wint[k];
+      }
+      const uint32_t n1 = run & 1023u, n2 = (run >> 10) & 1023u, n3 = run >> 20;
+      bbase[0] = n1 ? atomicAdd(counters + 1, (unsigned long long)n1) : 0;
+      bbase[1] = n2 ? atomicAdd(counters + 2, (unsigned long long)n2) : 0;
+      bbase[2] = n3 ? atomicAdd(counters + 0, (unsigned long long)n3) : 0;
+      if (tot) atomicAdd(counters + 3, tot);
+    }
+    __syncthreads();
+    const uint32_t off = wsum[warp] + incl - mine;
     if (kind == 1) {
-      unsigned long long dst = b1 + off;
+      const unsigned long long dst = bbase[0] + (off & 1023u);
       if ((int64_t)dst < m2l_cap) m2l[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
       else counters[4] = 1;
-    }
-    unsigned long long b2 = warp_reserve(counters + 2, kind == 2, off);
-    if (kind == 2) {
-      unsigned long long dst = b2 + off;
+    } else if (kind == 2) {
+      const unsigned long long dst = bbase[1] + ((off >> 10) & 1023u);
       if ((int64_t)dst < p2p_cap) p2p[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
       else counters[4] = 1;
-    }
-    unsigned long long b3 = warp_reserve(counters + 0, (kind >= 3) ? 8u : 0u, off);
-    if (kind >= 3) {
-      unsigned long long dst = b3 + off;
+    } else if (kind >= 3) {
+      const unsigned long long dst = bbase[2] + (off >> 20);
       if ((int64_t)(dst + 8) <= next_cap) {
+        int4 *o4 = reinterpret_cast<int4 *>(next + dst);  // dst is a multiple of 8
         if (kind == 3) {
-          const int c0 = c.child[t];
 #pragma unroll
-          for (int k = 0; k < 8; k++) next[dst + k] = make_int2(c0 + k, s);
+          for (int k = 0; k < 8; k += 2)
+            o4[k / 2] = make_int4(split_child + k, s, split_child + k + 1, s);
         } else {
-          const int c0 = c.child[s];
 #pragma unroll
-          for (int k = 0; k < 8; k++) next[dst + k] = make_int2(t, c0 + k);
+          for (int k = 0; k < 8; k += 2)
+            o4[k / 2] = make_int4(t, split_child + k, t, split_child + k + 1);
         }
       } else {
         counters[4] = 1;
       }
     }
-    // p2p interaction count
-    unsigned long long w = inter;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
-    if ((threadIdx.x & 31) == 0 && w) atomicAdd(counters + 3, w);
+    __syncthreads();  // wsum / bbase are rewritten by the next round
   }
 }
 
@@ -167,18 +189,126 @@ __global__ void pack_pairs(uint64_t *__restrict__ v, int64_t n, int b) {
   }
 }
 
-// off[c] = lower_bound(sorted packed keys, c << b), c in [0, ncells].
-__global__ void csr_offsets(const uint64_t *__restrict__ v, int64_t n, int b, int64_t ncells,
-                            int32_t *__restrict__ off) {
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t key = (uint64_t)c << b;
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-      int64_t mid = lo + ((hi - lo) >> 1);
-      if (v[mid] < key) lo = mid + 1; else hi = mid;
+// ---------------------------------------------------------------------------
+// List ordering.  The traversal emits pairs in an order set by its atomics;
+// the lists are put in (target, source) order by a counting sort on the
+// target (the counts' scan is the lists' CSR offsets) followed by a bitonic
+// sort of each target's sources in shared memory: one warp per segment of up
+// to kWarpSegMax pairs, one block per longer segment up to kSegSortMax, and
+// the radix sort of the whole list when a segment is longer still.  Every
+// (target, source) pair is visited at most once (the split rule is a function
+// of the pair, so two visiting paths from (root, root) cannot diverge), so a
+// segment's sources are distinct.
+// ---------------------------------------------------------------------------
+constexpr int kWarpSegMax = 512;
+constexpr int kSegSortMax = 8192;
+constexpr int kSegWarps = 8;
+constexpr int kLongThreads = 1024;
+
+__global__ void target_counts(const uint64_t *__restrict__ v, int64_t n, int32_t *__restrict__ cnt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + (v[i] >> 32), 1);
+}
+
+// *mx = max over c of off[c + 1] - off[c].
+__global__ void segment_max(const int32_t *__restrict__ off, int64_t ncells,
+                            unsigned long long *__restrict__ mx) {
+  unsigned m = 0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, (unsigned)(off[c + 1] - off[c]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(mx, (unsigned long long)m);
+}
+
+// Places each pair's source in its target's segment (order inside it
+// arbitrary).  cur starts as the segment offsets.
+__global__ void scatter_by_target(const uint64_t *__restrict__ v, int64_t n,
+                                  int32_t *__restrict__ cur, uint32_t *__restrict__ src) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t x = v[i];
+    const int32_t pos = atomicAdd(cur + (x >> 32), 1);
+    src[pos] = (uint32_t)x;
+  }
+}
+
+// Ascending bitonic sort of a[0, np), np a power of two, by threads
+// tid = 0 .. nthr-1 of a warp (kBlockLevel false) or of the block.
+template <bool kBlockLevel>
+__device__ __forceinline__ void bitonic_sort(uint32_t *a, int np, int tid, int nthr) {
+  for (int k = 2; k <= np; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int c = tid; c < (np >> 1); c += nthr) {
+        const int lo = ((c & ~(j - 1)) << 1) | (c & (j - 1));
+        const int hi = lo + j;
+        const uint32_t x = a[lo], y = a[hi];
+        if ((x > y) == ((lo & k) == 0)) {
+          a[lo] = y;
+          a[hi] = x;
+        }
+      }
+      if (kBlockLevel) __syncthreads(); else __syncwarp();
     }
-    off[c] = (int32_t)lo;
+  }
+}
+
+__device__ __forceinline__ int pow2_at_least(int n) {
+  int p = 2;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// One warp per target segment of at most kWarpSegMax sources; longer segments
+// are listed for sort_long_segments.  out[i] = t << b | sorted source.
+__global__ void __launch_bounds__(kSegWarps * 32) sort_segments(
+    const uint32_t *__restrict__ src, const int32_t *__restrict__ off, int64_t ncells, int b,
+    uint64_t *__restrict__ out, int32_t *__restrict__ long_list,
+    unsigned long long *__restrict__ long_cnt) {
+  __shared__ uint32_t buf[kSegWarps][kWarpSegMax];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *a = buf[warp];
+  const int64_t warps = (int64_t)gridDim.x * kSegWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kSegWarps + warp; c < ncells; c += warps) {
+    const int32_t a0 = off[c], len = off[c + 1] - a0;
+    const uint64_t th = (uint64_t)c << b;
+    if (len == 0) continue;
+    if (len > kWarpSegMax) {
+      if (lane == 0) long_list[atomicAdd(long_cnt, 1ull)] = (int32_t)c;
+      continue;
+    }
+    if (len == 1) {
+      if (lane == 0) out[a0] = th | src[a0];
+      continue;
+    }
+    const int np = pow2_at_least(len);
+    for (int i = lane; i < np; i += 32) a[i] = i < len ? src[a0 + i] : 0xFFFFFFFFu;
+    __syncwarp();
+    bitonic_sort<false>(a, np, lane, 32);
+    for (int i = lane; i < len; i += 32) out[a0 + i] = th | a[i];
+    __syncwarp();
+  }
+}
+
+// One block per listed segment of kWarpSegMax < length <= kSegSortMax.
+__global__ void __launch_bounds__(kLongThreads) sort_long_segments(
+    const uint32_t *__restrict__ src, const int32_t *__restrict__ off, int b,
+    uint64_t *__restrict__ out, const int32_t *__restrict__ long_list,
+    const unsigned long long *__restrict__ long_cnt) {
+  __shared__ uint32_t a[kSegSortMax];
+  const int64_t nl = (int64_t)*long_cnt;
+  for (int64_t k = blockIdx.x; k < nl; k += gridDim.x) {
+    const int32_t c = long_list[k];
+    const int32_t a0 = off[c], len = off[c + 1] - a0;
+    const uint64_t th = (uint64_t)c << b;
+    const int np = pow2_at_least(len);
+    for (int i = threadIdx.x; i < np; i += kLongThreads) a[i] = i < len ? src[a0 + i] : 0xFFFFFFFFu;
+    __syncthreads();
+    bitonic_sort<true>(a, np, threadIdx.x, kLongThreads);
+    for (int i = threadIdx.x; i < len; i += kLongThreads) out[a0 + i] = th | a[i];
+    __syncthreads();
   }
 }
 
@@ -203,11 +333,13 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
   ctx->theta = theta;
   ctx->have_lists = false;
   const int64_t C = ctx->ncells;
-  TB_CUDA(ctx, ctx->cell_r.ensure(C + 1, s));
-  cell_radii<<<grid_for(C, kBlock), kBlock, 0, s>>>(C, ctx->cmin.p, ctx->cmax.p, theta,
-                                                    ctx->cell_r.p);
+  TB_CUDA(ctx, ctx->trav_geo.ensure(C + 1, s));
+  TB_CUDA(ctx, ctx->trav_meta.ensure(C + 1, s));
+  trav_cells<<<grid_for(C, kBlock), kBlock, 0, s>>>(C, ctx->cmin.p, ctx->cmax.p, ctx->ccen.p,
+                                                    ctx->cnb.p, ctx->cleaf.p, ctx->cchild.p, theta,
+                                                    ctx->trav_geo.p, ctx->trav_meta.p);
   TB_LAUNCH_CHECK(ctx);
-  CellView cv{ctx->cleaf.p, ctx->cnb.p, ctx->cchild.p, ctx->ccen.p, ctx->cell_r.p};
+  const TravCells cv{ctx->trav_geo.p, ctx->trav_meta.p};
   TB_CUDA(ctx, ctx->counters.ensure(8, s));
   TB_CUDA(ctx, ctx->pinned.ensure(256));
   unsigned long long *hc = reinterpret_cast<unsigned long long *>(ctx->pinned.p);
@@ -217,15 +349,16 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     TB_CUDA(ctx, ctx->front_a.ensure(1024, s));
     const int2 root = make_int2(0, 0);
     TB_CUDA(ctx, cudaMemcpyAsync(ctx->front_a.p, &root, sizeof(int2), cudaMemcpyHostToDevice, s));
-    int64_t nfront = 1, n_m2l = 0, n_p2p = 0;
+    int64_t nfront = 1, n_m2l = 0, n_p2p = 0, visited = 0;
     int iters = 0;
     while (nfront > 0) {
+      visited += nfront;
       TB_CUDA(ctx, ctx->front_b.ensure(8 * nfront, s));
       TB_CUDA(ctx, ctx->m2l.ensure(n_m2l + nfront, s, true, n_m2l));
       TB_CUDA(ctx, ctx->p2p.ensure(n_p2p + nfront, s, true, n_p2p));
       TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s));
       dtt_step<<<grid_for(nfront, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-          cv, theta, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
+          cv, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
           (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p,
           ctx->reference_lists ? 0 : 1);
       TB_LAUNCH_CHECK(ctx);
@@ -249,6 +382,7 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     ctx->n_p2p = n_p2p;
     ctx->n_p2p_int = hc[3];
     ctx->trav_iters = iters;
+    ctx->trav_pairs = visited;
   }
   {
     PhaseTimer tm(ctx, &ctx->timings.list_sort);
@@ -256,11 +390,50 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     ctx->list_shift = b;
     TB_CUDA(ctx, ctx->m2l_off.ensure(C + 1, s));
     TB_CUDA(ctx, ctx->p2p_off.ensure(C + 1, s));
-    for (int which = 0; which < 2; which++) {
-      tb::DBuf<uint64_t> &L = which == 0 ? ctx->m2l : ctx->p2p;
-      tb::DBuf<int32_t> &off = which == 0 ? ctx->m2l_off : ctx->p2p_off;
-      const int64_t n = which == 0 ? ctx->n_m2l : ctx->n_p2p;
-      if (n > 0) {
+    TB_CUDA(ctx, ctx->list_cnt.ensure(C + 1, s));
+    const int64_t nlist[2] = {ctx->n_m2l, ctx->n_p2p};
+    tb::DBuf<uint64_t> *lists[2] = {&ctx->m2l, &ctx->p2p};
+    tb::DBuf<int32_t> *offs[2] = {&ctx->m2l_off, &ctx->p2p_off};
+    // 1. per-target counts -> CSR offsets, and the longest segment
+    TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p + 5, 0, 2 * sizeof(unsigned long long), s));
+    for (int w = 0; w < 2; w++) {
+      TB_CUDA(ctx, cudaMemsetAsync(ctx->list_cnt.p, 0, sizeof(int32_t) * (C + 1), s));
+      if (nlist[w] > 0) {
+        target_counts<<<grid_for(nlist[w], kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
+            lists[w]->p, nlist[w], ctx->list_cnt.p);
+        TB_LAUNCH_CHECK(ctx);
+      }
+      TB_TRY(scan_exclusive(ctx, ctx->list_cnt.p, offs[w]->p, C, offs[w]->p + C));
+      segment_max<<<grid_for(C, kBlock, ctx->num_sms * 8), kBlock, 0, s>>>(offs[w]->p, C,
+                                                                          ctx->counters.p + 5 + w);
+      TB_LAUNCH_CHECK(ctx);
+    }
+    TB_CUDA(ctx, cudaMemcpyAsync(hc + 5, ctx->counters.p + 5, 2 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaStreamSynchronize(s));
+    // 2. counting sort by target, then each target's sources
+    for (int w = 0; w < 2; w++) {
+      tb::DBuf<uint64_t> &L = *lists[w];
+      const int64_t n = nlist[w];
+      if (n == 0) continue;
+      if (hc[5 + w] <= (unsigned long long)kSegSortMax) {
+        TB_CUDA(ctx, ctx->list_src.ensure(n + 1, s));
+        TB_CUDA(ctx, cudaMemcpyAsync(ctx->list_cnt.p, offs[w]->p, sizeof(int32_t) * C,
+                                     cudaMemcpyDeviceToDevice, s));
+        TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p + 7, 0, sizeof(unsigned long long), s));
+        scatter_by_target<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
+            L.p, n, ctx->list_cnt.p, ctx->list_src.p);
+        TB_LAUNCH_CHECK(ctx);
+        // the per-target cursors are spent: their buffer holds the long-segment list
+        sort_segments<<<grid_for(C, kSegWarps, ctx->num_sms * 8), kSegWarps * 32, 0, s>>>(
+            ctx->list_src.p, offs[w]->p, C, b, L.p, ctx->list_cnt.p, ctx->counters.p + 7);
+        TB_LAUNCH_CHECK(ctx);
+        if (hc[5 + w] > (unsigned long long)kWarpSegMax) {
+          sort_long_segments<<<ctx->num_sms, kLongThreads, 0, s>>>(
+              ctx->list_src.p, offs[w]->p, b, L.p, ctx->list_cnt.p, ctx->counters.p + 7);
+          TB_LAUNCH_CHECK(ctx);
+        }
+      } else {
         TB_CUDA(ctx, ctx->list_alt.ensure(n + 1, s));
         pack_pairs<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.p, n, b);
         TB_LAUNCH_CHECK(ctx);
@@ -272,8 +445,6 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
           std::swap(L.cap, ctx->list_alt.cap);
         }
       }
-      csr_offsets<<<grid_for(C + 1, kBlock), kBlock, 0, s>>>(L.p, n, b, C, off.p);
-      TB_LAUNCH_CHECK(ctx);
     }
   }
   ctx->have_lists = true;

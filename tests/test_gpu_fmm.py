@@ -301,6 +301,42 @@ def test_device_pointers(tb, ctx):
     assert np.array_equal(out.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("ncrit,nsparse,longest", [(64, 120, 4000), (8, 16, 30000)],
+                         ids=["block-sorted", "radix-sorted"])
+def test_long_list_segments(tb, oracle_mod, ctx, ncrit, nsparse, longest):
+    """Leaves of a sparse half-cube beside a dense half each have a P2P list of
+    thousands of small leaves: longer than one warp sorts (a block sorts
+    them), or longer than one block sorts (the whole list goes through the
+    radix sort).  Both lists must still equal the reference traversal's as
+    sets, in (target, source) order."""
+    rng = np.random.default_rng(11)
+    dense = rng.random((120000, 3))
+    dense[:, 0] *= 0.5
+    sparse = rng.random((nsparse, 3))
+    sparse[:, 0] = 0.5 + 0.5 * sparse[:, 0]
+    pts = np.vstack([dense, sparse])
+    x, y, z = (np.ascontiguousarray(pts[:, d]) for d in range(3))
+    q = rng.random(len(x)) / len(x)
+    o = oracle_mod.Oracle(x, y, z, q, P=4, ncrit=ncrit, theta=0.3, run=False)
+    assert oracle_mod.lib().oracle_build(o.h) == 0
+    assert oracle_mod.lib().oracle_traverse(o.h) == 0
+    ctx.partition(x, y, z, q, ncrit=ncrit)
+    ctx.set_reference_lists(True)
+    try:
+        ctx.build_lists(0.3)
+        (gmt, gms), (gpt, gps) = ctx.lists()
+    finally:
+        ctx.set_reference_lists(False)
+    assert np.bincount(gpt).max() > longest  # the path is exercised
+    gkeys, okeys = ctx.cells()["key"], o.cells()["key"]
+    omt, oms = o.m2l_list()
+    opt, ops = o.p2p_list()
+    assert _pair_keys(gkeys, gmt, gms) == _pair_keys(okeys, omt, oms)
+    assert _pair_keys(gkeys, gpt, gps) == _pair_keys(okeys, opt, ops)
+    for t, s in ((gmt, gms), (gpt, gps)):
+        assert np.all(np.diff(t.astype(np.int64) * (1 << 32) + s) > 0)
+
+
 def test_long_source_lists_are_split(tb, ctx):
     """A Plummer set has leaves whose near-field lists hold far more than the
     32,768 source bodies one P2P work item takes; those lists are cut into
