@@ -32,6 +32,8 @@ HERE = pathlib.Path(__file__).resolve().parent
 MODEL_PATH = HERE / "chooser_model.npz"
 
 FIXED = {"P": 10, "theta": 0.4, "ncrit": 64, "precision": "fp64"}
+# log10 N of the training systems: 1e4 .. 1.6e7 bodies
+LOG10_N_MIN, LOG10_N_MAX = 4.0, float(np.log10(1.6e7))
 NBINS = 16
 FEATURE_NCRIT = 64
 
@@ -108,11 +110,11 @@ class LearnedChooser:
     def choose(self, features: np.ndarray, tol: float, precisions=(0, 1)) -> dict:
         g = candidate_grid()
         g = g[np.isin(g[:, 3], precisions)]
-        # Rank with log10 N inside the training range [4, 6]: the choice only
+        # Rank with log10 N inside the training range: the choice only
         # compares candidates for one system, so relative costs suffice and
         # the network is not asked to extrapolate in N.
         f = np.array(features, dtype=np.float64)
-        f[0] = min(max(f[0], 4.0), 6.0)
+        f[0] = min(max(f[0], LOG10_N_MIN), LOG10_N_MAX)
         pred = self.predict(encode(f, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
         ok = pred[:, 0] + self.margin <= np.log10(tol)
         if ok.any():
@@ -137,7 +139,7 @@ class LearnedChooser:
         g = candidate_grid()
         g = g[np.isin(g[:, 3], precisions)]
         f = np.array(features, dtype=np.float64)
-        f[0] = min(max(f[0], 4.0), 6.0)
+        f[0] = min(max(f[0], LOG10_N_MIN), LOG10_N_MAX)
         pred = self.predict(encode(f, g[:, 0], g[:, 1], g[:, 2], g[:, 3]))
         safe = self.choose(features, tol, precisions)
         out = []

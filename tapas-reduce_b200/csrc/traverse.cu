@@ -64,7 +64,8 @@ constexpr int kWarpsPerBlock = kBlock / 32;
 static_assert(kBlock <= 256, "packed per-block counts hold at most 256 threads");
 
 // counters: [0] next frontier size, [1] m2l size, [2] p2p size,
-//           [3] p2p body-pair interactions, [4] overflow flag
+//           [3] p2p body-pair interactions, [4] overflow bits (1: a list,
+//           2: the next frontier; [0] still counts the frontier's full size)
 // Slots in the three outputs are reserved once per block (one atomic per
 // counter per block), the block's threads taking consecutive slots.
 __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__restrict__ front,
@@ -154,11 +155,11 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
     if (kind == 1) {
       const unsigned long long dst = bbase[0] + (off & 1023u);
       if ((int64_t)dst < m2l_cap) m2l[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
-      else counters[4] = 1;
+      else atomicOr(counters + 4, 1ull);
     } else if (kind == 2) {
       const unsigned long long dst = bbase[1] + ((off >> 10) & 1023u);
       if ((int64_t)dst < p2p_cap) p2p[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
-      else counters[4] = 1;
+      else atomicOr(counters + 4, 1ull);
     } else if (kind >= 3) {
       const unsigned long long dst = bbase[2] + (off >> 20);
       if ((int64_t)(dst + 8) <= next_cap) {
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
             o4[k / 2] = make_int4(t, split_child + k, t, split_child + k + 1);
         }
       } else {
-        counters[4] = 1;
+        atomicOr(counters + 4, 2ull);
       }
     }
     __syncthreads();  // wsum / bbase are rewritten by the next round
@@ -350,28 +351,48 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     const int2 root = make_int2(0, 0);
     TB_CUDA(ctx, cudaMemcpyAsync(ctx->front_a.p, &root, sizeof(int2), cudaMemcpyHostToDevice, s));
     int64_t nfront = 1, n_m2l = 0, n_p2p = 0, visited = 0;
+    unsigned long long n_int = 0;
     int iters = 0;
+    unsigned long long *hset = hc + 16;  // counter values restored before a step
     while (nfront > 0) {
       visited += nfront;
-      TB_CUDA(ctx, ctx->front_b.ensure(8 * nfront, s));
+      // Each visited pair adds at most one M2L or P2P pair; the next frontier
+      // gets 2 * nfront slots first, and a step that needs more is run again
+      // with the size its reservations counted.
       TB_CUDA(ctx, ctx->m2l.ensure(n_m2l + nfront, s, true, n_m2l));
       TB_CUDA(ctx, ctx->p2p.ensure(n_p2p + nfront, s, true, n_p2p));
-      TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s));
-      dtt_step<<<grid_for(nfront, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-          cv, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
-          (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p,
-          ctx->reference_lists ? 0 : 1);
-      TB_LAUNCH_CHECK(ctx);
-      TB_CUDA(ctx, cudaMemcpyAsync(hc, ctx->counters.p, 5 * sizeof(unsigned long long),
-                                   cudaMemcpyDeviceToHost, s));
-      TB_CUDA(ctx, cudaStreamSynchronize(s));
-      if (hc[4]) {
-        set_error(ctx, "traversal: work list capacity exceeded");
-        return TAPAS_B200_ERR_CAPACITY;
+      TB_CUDA(ctx, ctx->front_b.ensure(std::max<int64_t>(2 * nfront, 1024), s));
+      for (int attempt = 0;; attempt++) {
+        hset[0] = 0;
+        hset[1] = (unsigned long long)n_m2l;
+        hset[2] = (unsigned long long)n_p2p;
+        hset[3] = n_int;
+        hset[4] = 0;
+        TB_CUDA(ctx, cudaMemcpyAsync(ctx->counters.p, hset, 5 * sizeof(unsigned long long),
+                                     cudaMemcpyHostToDevice, s));
+        dtt_step<<<grid_for(nfront, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
+            cv, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
+            (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p,
+            ctx->reference_lists ? 0 : 1);
+        TB_LAUNCH_CHECK(ctx);
+        TB_CUDA(ctx, cudaMemcpyAsync(hc, ctx->counters.p, 5 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s));
+        TB_CUDA(ctx, cudaStreamSynchronize(s));
+        if (hc[4] & 1) {
+          set_error(ctx, "traversal: work list capacity exceeded");
+          return TAPAS_B200_ERR_CAPACITY;
+        }
+        if (!(hc[4] & 2)) break;
+        if (attempt > 0) {
+          set_error(ctx, "traversal: frontier capacity exceeded after resizing");
+          return TAPAS_B200_ERR_CAPACITY;
+        }
+        TB_CUDA(ctx, ctx->front_b.ensure((size_t)hc[0], s));
       }
       nfront = (int64_t)hc[0];
       n_m2l = (int64_t)hc[1];
       n_p2p = (int64_t)hc[2];
+      n_int = hc[3];
       std::swap(ctx->front_a, ctx->front_b);
       if (++iters > 4 * (kMaxDepth + 2)) {
         set_error(ctx, "traversal did not terminate within its iteration bound");
@@ -380,7 +401,7 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     }
     ctx->n_m2l = n_m2l;
     ctx->n_p2p = n_p2p;
-    ctx->n_p2p_int = hc[3];
+    ctx->n_p2p_int = n_int;
     ctx->trav_iters = iters;
     ctx->trav_pairs = visited;
   }

@@ -1,15 +1,16 @@
 """Data generation, training and held-out evaluation of the learned chooser.
 
 Run on a GPU, from the repository root:
-    python tapas-reduce_b200/train_chooser.py generate   # 2,000 FMM runs -> chooser_data.npz
+    python tapas-reduce_b200/train_chooser.py generate   # 2,320 FMM runs -> chooser_data.npz
     python tapas-reduce_b200/train_chooser.py train      # own CUDA kernels -> chooser_model.npz
     python tapas-reduce_b200/train_chooser.py evaluate   # 200 held-out systems
 
-Training systems: 250 seeded body sets, N log-uniform in [1e4, 1e6], the
+Training systems: 250 seeded body sets, N log-uniform in [1e4, 1e6], and 40
+with N log-uniform in [1e6, 1.6e7] (theta >= 0.25, ncrit >= 32), the
 distribution drawn from {uniform cube [-1,1]^3, Plummer, two Gaussian clusters
 sigma 0.1 with centres 1.0 apart, unit sphere surface}, charges equal positive
 or zero-mean U[-1,1] with equal odds; 8 random settings each (P in 4..16, theta in [0.2, 0.7], ncrit in
-{16, 32, 64, 128}, mixed or FP64) = 2,000 runs.  Each run records the
+{16, 32, 64, 128}, mixed or FP64) = 2,320 runs.  Each run records the
 relative-L2 potential error against an FP64 direct sum on 256 sampled targets
 and the device time of the evaluation (sum of the library's CUDA-event phase
 timings: tree, upward, traversal, M2L, P2P, downward).
@@ -43,9 +44,9 @@ def _pkg():
     return mod
 
 
-def make_system(tb, i, seed_base):
+def make_system(tb, i, seed_base, log10_n=(4.0, 6.0)):
     rng = np.random.default_rng(seed_base + i)
-    n = int(round(10 ** rng.uniform(4, 6)))
+    n = int(round(10 ** rng.uniform(*log10_n)))
     dist = DISTS[int(rng.integers(len(DISTS)))]
     x, y, z, _ = tb.datasets.make(dist, n, seed_base + i)
     if rng.random() < 0.5:  # zero-mean charges
@@ -65,29 +66,43 @@ def timed_run(tb, ctx, bodies, P, theta, ncrit, prec):
     return res, float(sum(t[k] for k in PHASES))
 
 
-def generate(n_systems=250, per_system=8, seed_base=10_000, out=DATA_PATH):
+def generate(n_systems=250, per_system=8, seed_base=10_000, out=DATA_PATH, n_large=40):
+    """n_systems body sets of 1e4..1e6 bodies, then n_large of 1e6..1.6e7 (the
+    large runs keep theta >= 0.25 and ncrit >= 32, so every run's lists stay
+    within a few GB)."""
     tb = _pkg()
     from tapas_reduce_b200 import chooser, verify
     rows = []
+    sets = [(i, seed_base, (4.0, 6.0)) for i in range(n_systems)]
+    sets += [(i, seed_base + 50_000, (6.0, chooser.LOG10_N_MAX)) for i in range(n_large)]
     with tb.Context(0) as ctx:
-        for i in range(n_systems):
-            dist, n, bodies, rng = make_system(tb, i, seed_base)
+        for k, (i, base, log10_n) in enumerate(sets):
+            dist, n, bodies, rng = make_system(tb, i, base, log10_n)
+            large = n > 1_000_000
             feats = chooser.system_features(ctx, *bodies)
-            tg = tb.datasets.sample_targets(n, 256, seed=seed_base + i)
+            tg = tb.datasets.sample_targets(n, 256, seed=base + i)
             d = ctx.direct(tg)
             for _ in range(per_system):
-                P = int(rng.integers(4, 17))
-                theta = float(np.round(rng.uniform(0.2, 0.7), 2))
-                ncrit = int(rng.choice([16, 32, 64, 128]))
-                fp64 = int(rng.random() < 0.3)
-                res, ms = timed_run(tb, ctx, bodies, P, theta, ncrit,
-                                    tb.FP64 if fp64 else tb.MIXED)
+                for attempt in range(4):  # a setting too large for the device: draw again
+                    P = int(rng.integers(4, 17))
+                    theta = float(np.round(rng.uniform(0.25 if large else 0.2, 0.7), 2))
+                    ncrit = int(rng.choice([32, 64, 128] if large else [16, 32, 64, 128]))
+                    fp64 = int(rng.random() < 0.3)
+                    try:
+                        res, ms = timed_run(tb, ctx, bodies, P, theta, ncrit,
+                                            tb.FP64 if fp64 else tb.MIXED)
+                        break
+                    except tb.TapasError as err:
+                        print(f"system {k} n={n} {dist} P={P} theta={theta} ncrit={ncrit}: "
+                              f"{err}", flush=True)
+                        if attempt == 3:
+                            raise
                 err = verify.rel_l2(res[tg], d)[0]
                 rows.append(np.concatenate([feats, [P, theta, ncrit, fp64,
                                                     np.log10(max(err, 1e-16)),
                                                     np.log10(ms), n, DISTS.index(dist)]]))
-            if (i + 1) % 25 == 0:
-                print(f"{i + 1}/{n_systems} systems", flush=True)
+            if (k + 1) % 25 == 0:
+                print(f"{k + 1}/{len(sets)} systems", flush=True)
     data = np.array(rows)
     np.savez_compressed(out, data=data, nfeat=len(feats))
     print(f"wrote {out}: {data.shape}")
