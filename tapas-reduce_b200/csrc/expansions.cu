@@ -31,6 +31,37 @@ struct Sizes {
 // ---------------------------------------------------------------------------
 // P2M (:138-163): M[n,m] = sum_b q_b * conj(Y_n^m(x_b - center))
 // ---------------------------------------------------------------------------
+// Coefficient index t = n(n+1)/2 + m of position s in P2M's term order
+// (m = 0..P-1, then n = m..P-1).
+template <int P>
+__device__ __forceinline__ int p2m_term_index(int s) {
+  int m = 0;
+  while (s >= P - m) {
+    s -= P - m;
+    m++;
+  }
+  const int n = m + s;
+  return n * (n + 1) / 2 + m;
+}
+
+// Sums buf[0..15] of every lane over the warp, leaving lane l (and l ^ 1) with
+// the total of buf[(l >> 1) & 15]: four halving exchanges (each lane keeps the
+// half its lane bit selects and sends the other), then one pairwise add.
+// 16 + 8 + 4 + 2 values are exchanged instead of 16 separate 5-step sums.
+__device__ __forceinline__ double warp_reduce_scatter16(double (&buf)[16], int lane) {
+#pragma unroll
+  for (int o = 16, h = 8; o >= 2; o >>= 1, h >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; i++) {
+      const double keep = up ? buf[i + h] : buf[i];
+      const double send = up ? buf[i] : buf[i + h];
+      buf[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return buf[0] + __shfl_xor_sync(0xffffffffu, buf[0], 1);
+}
+
 template <int P>
 __global__ void __launch_bounds__(kThreads) p2m_kernel(
     const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
@@ -38,15 +69,17 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
     const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
     const double *__restrict__ sq, double2 *__restrict__ M) {
   using S = Sizes<P>;
+  constexpr int kGroups = (S::NT + 7) / 8;  // 8 complex terms per reduction
   const int lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
   if (w >= nleaves) return;
   const int c = leaves[w];
   const int b0 = cbeg[c], nb = cnb[c];
   const double cx = ccen[3 * c], cy = ccen[3 * c + 1], cz = ccen[3 * c + 2];
-  cd acc[S::R];
+  // acc[g]: this lane's share of group g's sums, component (lane >> 1) & 15
+  double acc[kGroups];
 #pragma unroll
-  for (int r = 0; r < S::R; r++) acc[r] = cd{0, 0};
+  for (int g = 0; g < kGroups; g++) acc[g] = 0;
   for (int base = 0; base < nb; base += 32) {
     const int b = base + lane;
     const bool valid = b < nb;
@@ -59,8 +92,10 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
     double sb, cb;
     sincos(beta, &sb, &cb);
     const cd ei{cb, sb};
-    // Streamed evalMultipole (:63-99); each (n, m>=0) term q*conj(Y_n^m) is
-    // summed over the warp's bodies and kept by lane t%32.
+    // Streamed evalMultipole (:63-99): this body's q*conj(Y_n^m) terms, 8 at a
+    // time, summed over the warp's bodies by one reduce-scatter.
+    double buf[16];
+    int s = 0;
     double fact = 1, pn = 1, rhom = 1;
     cd eim{1.0, 0.0};
 #pragma unroll
@@ -71,17 +106,14 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
       for (int n = m; n < P; n++) {
         if (n > m) rhon *= 1.0 / -(n + m);  // constants after unrolling
         const double sc = q * rhon * p;
-        double vx = sc * eim.x, vy = -sc * eim.y;
+        buf[2 * (s & 7)] = sc * eim.x;
+        buf[2 * (s & 7) + 1] = -sc * eim.y;
+        if ((s & 7) == 7 || s == S::NT - 1) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          vx += __shfl_xor_sync(0xffffffffu, vx, o);
-          vy += __shfl_xor_sync(0xffffffffu, vy, o);
+          for (int i = 2 * (s & 7) + 2; i < 16; i++) buf[i] = 0;
+          acc[s >> 3] += warp_reduce_scatter16(buf, lane);
         }
-        const int t = n * (n + 1) / 2 + m;
-        if (lane == (t & 31)) {
-          acc[t >> 5].x += vx;
-          acc[t >> 5].y += vy;
-        }
+        s++;
         if (n == m) {
           p = x * (2 * m + 1) * p1;
           rhon = rhom * rho;
@@ -98,11 +130,14 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
       eim = cmul(eim, ei);
     }
   }
-  double2 *Mc = M + (int64_t)c * S::NT;
+  double *Mc = reinterpret_cast<double *>(M + (int64_t)c * S::NT);
+  const int d = (lane >> 1) & 15;
+  if ((lane & 1) == 0) {
 #pragma unroll
-  for (int r = 0; r < S::R; r++) {
-    const int t = lane + 32 * r;
-    if (t < S::NT) Mc[t] = make_double2(acc[r].x, acc[r].y);
+    for (int g = 0; g < kGroups; g++) {
+      const int sp = 8 * g + (d >> 1);
+      if (sp < S::NT) Mc[2 * p2m_term_index<P>(sp) + (d & 1)] = acc[g];
+    }
   }
 }
 
@@ -326,17 +361,22 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
     double pot = 0, s0 = 0, s1 = 0, s2 = 0;
     double fact = 1, pn = 1, rhom = 1;
     cd eim{1.0, 0.0};
+    // For each m the sums over n are taken before the common factor e^{im phi}:
+    //   sa = sum ys L, sb = sum n ys L, sc = sum (yts / inv_y) L,
+    // where Y_n^m = ys e^{im phi} and dY_n^m/dtheta = yts e^{im phi}.
 #pragma unroll
     for (int m = 0; m < P; m++) {
       double p = pn, p1 = pn;
       double rhon = rhom;
+      cd sa{0, 0}, sb{0, 0}, sc{0, 0};
 #pragma unroll
       for (int n = m; n < P; n++) {
-        double ys, yts;  // Y_n^m = ys * e^{im phi}, dY/dtheta = yts * e^{im phi}
+        double ys, yt;
+        const double t1 = x * p1;
         if (n == m) {
-          const double pnew = x * (2 * m + 1) * p1;
+          const double pnew = (2 * m + 1) * t1;
           ys = rhom * p;
-          yts = rhom * (pnew - (m + 1) * x * p1) * inv_y;
+          yt = rhom * (pnew - (m + 1) * t1);
           p = pnew;
           rhon = rhom * r;
         } else {
@@ -344,19 +384,26 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
           ys = rhon * p;
           const double p2 = p1;
           p1 = p;
-          p = (x * (2 * n + 1) * p1 - (n + m) * p2) * (1.0 / (n - m + 1));
-          yts = rhon * ((n - m + 1) * p - (n + 1) * x * p1) * inv_y;
+          const double tn = x * p1;
+          p = ((2 * n + 1) * tn - (n + m) * p2) * (1.0 / (n - m + 1));
+          yt = rhon * ((n - m + 1) * p - (n + 1) * tn);
           rhon *= r;
         }
         const cd Lv = Lc[n * (n + 1) / 2 + m];
-        const cd LY = cmul(Lv, scal(ys, eim));
-        const cd LYt = cmul(Lv, scal(yts, eim));
-        const double f = (m == 0) ? 1.0 : 2.0;
-        pot += f * LY.x;
-        s0 += f * LY.x * inv_r * n;
-        s1 += f * LYt.x;
-        if (m > 0) s2 += 2 * (-LY.y) * m;  // real(L*Y*i) = -imag(L*Y)
+        sa.x = fma(ys, Lv.x, sa.x);
+        sa.y = fma(ys, Lv.y, sa.y);
+        const double nys = n * ys;
+        sb.x = fma(nys, Lv.x, sb.x);
+        sb.y = fma(nys, Lv.y, sb.y);
+        sc.x = fma(yt, Lv.x, sc.x);
+        sc.y = fma(yt, Lv.y, sc.y);
       }
+      const double f = (m == 0) ? 1.0 : 2.0;
+      const cd za = cmul(sa, eim);
+      pot += f * za.x;
+      s0 += f * inv_r * (sb.x * eim.x - sb.y * eim.y);
+      s1 += f * inv_y * (sc.x * eim.x - sc.y * eim.y);
+      if (m > 0) s2 += 2 * (-za.y) * m;  // real(L*Y*i) = -imag(L*Y)
       rhom = rhom * r * (1.0 / (double)(-(2 * m + 2) * (2 * m + 1)));
       pn = -pn * fact * y;
       fact += 2;
