@@ -188,6 +188,9 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->list_src.release();
   ctx->M.release();
   ctx->L.release();
+  ctx->op_m2m.release();
+  ctx->op_l2l.release();
+  ctx->op_part.release();
   mixed_release(ctx);
   mlp_release(ctx);
   ctx->bh_attr.release();

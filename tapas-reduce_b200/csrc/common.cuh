@@ -200,6 +200,9 @@ struct tapas_b200_ctx {
   size_t tc_op_budget = (size_t)4 << 30;  // bytes of split-TF32 operators kept at once
   bool have_M = false, have_L = false;
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
+  tb::DBuf<double> op_m2m, op_l2l;      // per level: child<->parent translation operators
+  int level_ops_P = 0;                  // order the operators were built for (0: none)
+  tb::DBuf<double> op_part;             // M2M of small levels: per-octant partial products
 
   tb::Mlp *mlp = nullptr;               // learned chooser network, if created
 

@@ -1,17 +1,17 @@
 // FP64 expansion kernels: P2M, M2M, M2L, L2L, L2P (ExaFMM Laplace spherical
 // harmonics, ex/LaplaceSphericalCPU_tapas.h), templated on the order P.
 //
-// Work mapping (one warp per cell; the warp's lanes split the expansion
-// coefficients, the harmonics table of each translation is built by P lanes,
-// one Legendre column per lane, into the warp's shared-memory slice):
-//   P2M  - warp per non-empty leaf; lanes own bodies, each (n,m) term is a
-//          warp shuffle reduction, lane t%32 keeps coefficient t.
-//   M2M  - per level, bottom-up; warp per non-leaf cell, 8 children.
-//   M2L  - warp per target cell over its CSR list of sources.
-//   L2L  - per level, top-down; warp per non-empty cell.
+// Work mapping:
+//   P2M  - warp per non-empty leaf; lanes own bodies; 8 coefficients at a time
+//          are summed over the warp by one reduce-scatter.
+//   M2M  - per level, one FP64 GEMM of the level's precomputed translation
+//          operator with the stacked multipoles of the children (below).
+//   M2L  - warp per target cell over its CSR list of sources; the harmonics
+//          table of each translation is built by P lanes, one Legendre
+//          column per lane, into the warp's shared-memory slice.
+//   L2L  - per level, one FP64 GEMM as M2M, parents to stacked children.
 //   L2P  - warp per non-empty leaf; lane per body, harmonics streamed in
 //          registers (no table), L of the leaf staged in shared memory.
-// Bound: FP64 pipe (M2L ~ 8 sum_j (j+1)(P-j)^2 flop per translation).
 #include "expansions.cuh"
 #include "kernels.cuh"
 
@@ -142,74 +142,6 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// M2M (:165-206), one level: M[c] = sum over 8 children of the shifted M.
-// ---------------------------------------------------------------------------
-template <int P>
-__global__ void __launch_bounds__(kThreads) m2m_kernel(
-    int64_t a, int64_t cnt, const int32_t *__restrict__ cleaf, const int32_t *__restrict__ cnb,
-    const int32_t *__restrict__ cchild, const double *__restrict__ ccen, double2 *__restrict__ M) {
-  using S = Sizes<P>;
-  __shared__ cd Ysm[kWarps][S::NY];
-  __shared__ cd Msm[kWarps][S::NT];
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-  const int64_t w = (int64_t)blockIdx.x * kWarps + wi;
-  if (w >= cnt) return;
-  const int64_t c = a + w;
-  if (cleaf[c] || cnb[c] == 0) return;  // an empty cell's M stays zero
-  cd *Y = Ysm[wi];
-  cd *Mj = Msm[wi];
-  cd acc[S::R];
-  int jj[S::R], kk[S::R];
-#pragma unroll
-  for (int r = 0; r < S::R; r++) {
-    acc[r] = cd{0, 0};
-    jk_of(lane + 32 * r, jj[r], kk[r]);
-  }
-  const int ch0 = cchild[c];
-  for (int ci = 0; ci < 8; ci++) {
-    const int cj = ch0 + ci;
-    if (cnb[cj] == 0) continue;  // an empty child's M is zero
-    const Sph sp = sph_of(ccen[3 * c] - ccen[3 * cj], ccen[3 * c + 1] - ccen[3 * cj + 1],
-                          ccen[3 * c + 2] - ccen[3 * cj + 2]);
-    __syncwarp();
-    if (lane < P) multipole_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
-    for (int t = lane; t < S::NT; t += 32) {
-      double2 v = M[(int64_t)cj * S::NT + t];
-      Mj[t] = cd{v.x, v.y};
-    }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < S::R; r++) {
-      if (lane + 32 * r >= S::NT) continue;
-      const int j = jj[r], k = kk[r];
-      cd m_acc{0, 0};
-      for (int n = 0; n <= j; n++) {
-        const int mlo = max(-n, -j + k + n), mhi = min(k - 1, n);
-        for (int m = mlo; m <= mhi; m++) {
-          const int jnkms = (j - n) * (j - n + 1) / 2 + k - m;
-          const int nm = n * n + n - m;
-          const double sgn = ((m >= 0) ? 1.0 : oddeven(m)) * oddeven(n);
-          cmac(m_acc, scal(sgn, Mj[jnkms]), Y[nm]);
-        }
-        const int mhi2 = min(n, j + k - n);
-        for (int m = k; m <= mhi2; m++) {
-          const int jnkms = (j - n) * (j - n + 1) / 2 - k + m;
-          const int nm = n * n + n - m;
-          cmac(m_acc, scal(oddeven(k + n + m), conjd(Mj[jnkms])), Y[nm]);
-        }
-      }
-      acc[r].x += m_acc.x;
-      acc[r].y += m_acc.y;
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < S::R; r++) {
-    const int t = lane + 32 * r;
-    if (t < S::NT) M[c * S::NT + t] = make_double2(acc[r].x, acc[r].y);
-  }
-}
-
-// ---------------------------------------------------------------------------
 // M2L (:208-273, mutual = 0): L[t] = sum over sources s of T(c_t - c_s) M[s]
 // ---------------------------------------------------------------------------
 template <int P>
@@ -270,57 +202,6 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
   for (int r = 0; r < S::R; r++) {
     const int t = lane + 32 * r;
     if (t < S::NT) L[c * S::NT + t] = make_double2(acc[r].x, acc[r].y);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// L2L (:309-345), one level: L[c] += shifted L[parent]
-// ---------------------------------------------------------------------------
-template <int P>
-__global__ void __launch_bounds__(kThreads) l2l_kernel(
-    int64_t a, int64_t cnt, const int32_t *__restrict__ cnb, const int32_t *__restrict__ cparent,
-    const double *__restrict__ ccen, double2 *__restrict__ L) {
-  using S = Sizes<P>;
-  __shared__ cd Ysm[kWarps][S::NY];
-  __shared__ cd Lsm[kWarps][S::NT];
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-  const int64_t w = (int64_t)blockIdx.x * kWarps + wi;
-  if (w >= cnt) return;
-  const int64_t c = a + w;
-  if (cnb[c] == 0) return;
-  const int p = cparent[c];
-  cd *Y = Ysm[wi];
-  cd *Lp = Lsm[wi];
-  const Sph sp = sph_of(ccen[3 * c] - ccen[3 * p], ccen[3 * c + 1] - ccen[3 * p + 1],
-                        ccen[3 * c + 2] - ccen[3 * p + 2]);
-  if (lane < P) multipole_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
-  for (int t = lane; t < S::NT; t += 32) {
-    double2 v = L[(int64_t)p * S::NT + t];
-    Lp[t] = cd{v.x, v.y};
-  }
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < S::R; r++) {
-    const int t = lane + 32 * r;
-    if (t >= S::NT) continue;
-    int j, k;
-    jk_of(t, j, k);
-    cd acc{0, 0};
-    for (int n = j; n < P; n++) {
-      const int base = (n - j) * (n - j) + n - j - k;
-      for (int m = j + k - n; m < 0; m++) {
-        const int nms = n * (n + 1) / 2 - m;
-        cmac(acc, scal(oddeven(k), conjd(Lp[nms])), Y[base + m]);
-      }
-      for (int m = 0; m <= n; m++) {
-        if (n - j >= abs(m - k)) {
-          const int nms = n * (n + 1) / 2 + m;
-          cmac(acc, scal(oddeven((m - k) * (m < k)), Lp[nms]), Y[base + m]);
-        }
-      }
-    }
-    double2 o = L[c * S::NT + t];
-    L[c * S::NT + t] = make_double2(o.x + acc.x, o.y + acc.y);
   }
 }
 
@@ -424,6 +305,311 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Level-batched M2M and L2L.
+//
+// Every cell of a level has the same width (the root cube halved per level),
+// so a child's offset from its parent is one of eight per level and the
+// translation of M2M (:165-206) or L2L (:309-345) is one fixed real-linear
+// map per (level, octant), acting on (Re, Im) pairs.  The eight children of
+// the non-leaf cells of a level are stored consecutively in parent order, so
+//   M2M:  M[parent_i]          = Tup_l (2NT x 16NT) . M[children_i] (16NT)
+//   L2L:  L[children_i] (16NT) += Tdn_l (16NT x 2NT) . L[parent_i]
+// are one FP64 GEMM per level over the level's non-leaf cells i.  The
+// operators are built from one representative parent of the level with the
+// reference's formulas, one thread per (target, source) block; M2M rows of degree j read only source degrees <= j
+// and L2L rows of degree j only source degrees >= j, and the GEMM skips the
+// zero ranges this leaves.
+// ---------------------------------------------------------------------------
+constexpr int kMaxLevels = kMaxDepth + 1;
+struct LevelFirstChild {
+  int64_t c0[kMaxLevels];  // first cell of level l + 1 (child 0 of the level's first parent)
+};
+
+__host__ __device__ __forceinline__ int degree_of(int t) {
+  int j = 0;
+  while ((j + 1) * (j + 2) / 2 <= t) j++;
+  return j;
+}
+
+// The real 2 x 2 block mapping a source coefficient to a target one when
+// out = a * src + b * conj(src):
+//   [Re out]   [a.x + b.x   b.y - a.y] [Re src]
+//   [Im out] = [a.y + b.y   a.x - b.x] [Im src]
+// stored transposed (operators are kept K x R, column k of the map
+// contiguous): colre / colim point at the target's two rows in the source's
+// real / imaginary column.
+__device__ __forceinline__ void store_block(double *colre, double *colim, cd a, cd b) {
+  *reinterpret_cast<double2 *>(colre) = make_double2(a.x + b.x, a.y + b.y);
+  *reinterpret_cast<double2 *>(colim) = make_double2(b.y - a.y, a.x - b.x);
+}
+
+// grid (levels with children, 8 octants, 2: M2M / L2L); every entry of the
+// operators is written.  Entry (target (j,k), source (j',k')) collects the
+// terms of the reference's loops that read that source: M2M (:165-206) with
+// n = j - j' and m = k - k' (source as is) or m = k + k' (conjugated); L2L
+// (:309-345) with n = j' and m = k' (as is) or m = -k' (conjugated).
+template <int P>
+__global__ void __launch_bounds__(256) build_translation_ops(
+    LevelFirstChild lf, const int32_t *__restrict__ cparent, const double *__restrict__ ccen,
+    double *__restrict__ op_up, double *__restrict__ op_dn) {
+  using S = Sizes<P>;
+  constexpr int NT2 = 2 * S::NT;
+  __shared__ cd Y[S::NY];
+  const int l = blockIdx.x, o = blockIdx.y;
+  const bool up = blockIdx.z == 0;
+  const int64_t cj = lf.c0[l] + o;
+  const int p = cparent[cj];
+  const double dx = ccen[3 * p] - ccen[3 * cj], dy = ccen[3 * p + 1] - ccen[3 * cj + 1],
+               dz = ccen[3 * p + 2] - ccen[3 * cj + 2];
+  // M2M translates by parent - child, L2L by child - parent
+  const Sph sp = up ? sph_of(dx, dy, dz) : sph_of(-dx, -dy, -dz);
+  if (threadIdx.x < P) multipole_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
+  __syncthreads();
+  for (int e = threadIdx.x; e < S::NT * S::NT; e += blockDim.x) {
+    const int u = e / S::NT, t = e - u * S::NT;  // consecutive threads: consecutive targets
+    int j, k, jp, kp;
+    jk_of(t, j, k);
+    jk_of(u, jp, kp);
+    cd a{0, 0}, b{0, 0};
+    if (up) {
+      const int n = j - jp;
+      if (n >= 0) {
+        if (kp >= 1) {
+          const int m = k - kp;
+          if (m >= -n && m <= n) {
+            const double sgn = ((m >= 0) ? 1.0 : oddeven(m)) * oddeven(n);
+            a = scal(sgn, Y[n * n + n - m]);
+          }
+        }
+        const int m = k + kp;
+        if (m <= n) b = scal(oddeven(k + n + m), Y[n * n + n - m]);
+      }
+      // K = 16 NT sources (child o's at o * 2NT), R = 2NT targets
+      double *c0 = op_up + (size_t)l * NT2 * 8 * NT2 + (size_t)(o * NT2 + 2 * u) * NT2 + 2 * t;
+      store_block(c0, c0 + NT2, a, b);
+    } else {
+      const int n = jp;
+      if (n >= j) {
+        const int base = (n - j) * (n - j) + n - j - k;
+        if (kp >= 1 && kp <= n - j - k) b = scal(oddeven(k), Y[base - kp]);
+        if (n - j >= abs(kp - k)) a = scal(oddeven((kp - k) * (kp < k)), Y[base + kp]);
+      }
+      // K = 2NT sources, R = 16 NT targets (child o's at o * 2NT)
+      double *c0 = op_dn + (size_t)l * 8 * NT2 * NT2 + (size_t)(2 * u) * (8 * NT2) + o * NT2 + 2 * t;
+      store_block(c0, c0 + 8 * NT2, a, b);
+    }
+  }
+}
+
+// One level's translation GEMM.  Column i is the level's i-th non-leaf cell:
+// its children are cells c0 + 8i .. c0 + 8i + 7, its index cparent[c0 + 8i].
+struct LevelGemm {
+  const double *At; // operator, transposed: K x R, row k = the map's column k
+  int R, K, nt2;    // nt2 = 2 NT
+  int up;           // 1: M2M (C = A B), 0: L2L (C += A B)
+  int split;        // M2M only: blockIdx.z = octant, partial products to `part`
+  int64_t c0, ncols;
+  const int32_t *cparent;
+  double *X;        // M (up) or L (down) as doubles, nt2 per cell
+  double *part;     // split: [8][ncols][R]
+};
+
+constexpr int kGM = 64, kGN = 64, kGK = 16, kGThreads = 256;
+
+// 64 x 64 output tile per block; warp w covers rows 32 (w & 1) + {2i, 2i+1,
+// 16+2i, 17+2i} (i = lane & 7) and columns 16 (w >> 1) + 4 (lane >> 3) .. +3,
+// so every shared-memory read of a warp is conflict-free.  A tiles are copied
+// as they lie (k-major); B tiles are loaded one column per lane.  The next
+// 16-source chunk is loaded into registers while the current one is
+// multiplied from shared memory (two buffers, one barrier per chunk).
+__global__ void __launch_bounds__(kGThreads, 3) level_gemm(LevelGemm g) {
+  __shared__ __align__(16) double As[2][kGK][kGM];
+  __shared__ __align__(16) double Bs[2][kGK][kGN];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int r0 = blockIdx.y * kGM;
+  const int64_t n0 = (int64_t)blockIdx.x * kGN;
+  const int wr = 32 * (w & 1) + 2 * (lane & 7);    // rows wr, wr+1, wr+16, wr+17
+  const int tc = 16 * (w >> 1) + 4 * (lane >> 3);  // columns tc .. tc+3
+  // A loads: rows r0 + 2 (tid & 31) (+1), sources (tid >> 5) and (tid >> 5) + 8
+  const int am = 2 * (tid & 31), ak = tid >> 5;
+  const bool arow_ok = r0 + am < g.R;  // R even: the pair is valid together
+  // B loads: column tid & 63, sources 4 (tid >> 6) .. +3
+  const int bn = tid & 63, bk = 4 * (tid >> 6);
+  const int64_t bcol_i = n0 + bn;
+  const bool bcol_ok = bcol_i < g.ncols;
+  const double *bcol = nullptr;
+  if (bcol_ok) {
+    const int64_t child0 = g.c0 + 8 * bcol_i;
+    const int64_t cell = g.up ? child0 : (int64_t)g.cparent[child0];
+    bcol = g.X + cell * g.nt2;
+  }
+  // source ranges holding the tile's nonzero operator columns
+  int seg0, nseg, seg_len, seg_k0;
+  if (g.up) {
+    const int tmax = (min(r0 + kGM, g.R) - 1) / 2;
+    const int jm = degree_of(tmax);
+    seg0 = g.split ? (int)blockIdx.z : 0;
+    nseg = g.split ? 1 : 8;
+    seg_len = min(g.nt2, (jm + 1) * (jm + 2));
+    seg_k0 = 0;
+  } else {
+    const int rs = r0 % g.nt2;
+    int kstart = 0;
+    if (rs + kGM <= g.nt2) {
+      const int j = degree_of(rs / 2);
+      kstart = j * (j + 1);
+    }
+    seg0 = 0;
+    nseg = 1;
+    seg_k0 = kstart;
+    seg_len = g.nt2 - kstart;
+  }
+  const int cps = (seg_len + kGK - 1) / kGK;  // chunks per segment
+  const int nchunks = nseg * cps;
+  double2 av[2], bv[2];
+  auto load_chunk = [&](int c) {
+    const int sg = seg0 + c / cps, kc = (c % cps) * kGK;
+    const int kseg = seg_k0 + sg * g.nt2;  // first source of the segment
+#pragma unroll
+    for (int x = 0; x < 2; x++) {
+      const int kk = kc + ak + 8 * x;
+      av[x] = (kk < seg_len && arow_ok)
+                  ? *reinterpret_cast<const double2 *>(g.At + (size_t)(kseg + kk) * g.R + r0 + am)
+                  : make_double2(0, 0);
+      const int kb = kc + bk + 2 * x;  // even; seg_len is even
+      bv[x] = (kb < seg_len && bcol_ok) ? *reinterpret_cast<const double2 *>(bcol + kseg + kb)
+                                        : make_double2(0, 0);
+    }
+  };
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0;
+  if (nchunks > 0) load_chunk(0);
+  for (int c = 0; c < nchunks; c++) {
+    const int buf = c & 1;
+#pragma unroll
+    for (int x = 0; x < 2; x++) {
+      *reinterpret_cast<double2 *>(&As[buf][ak + 8 * x][am]) = av[x];
+      Bs[buf][bk + 2 * x][bn] = bv[x].x;
+      Bs[buf][bk + 2 * x + 1][bn] = bv[x].y;
+    }
+    __syncthreads();
+    if (c + 1 < nchunks) load_chunk(c + 1);
+#pragma unroll
+    for (int k = 0; k < kGK; k++) {
+      const double2 a01 = *reinterpret_cast<const double2 *>(&As[buf][k][wr]);
+      const double2 a23 = *reinterpret_cast<const double2 *>(&As[buf][k][wr + 16]);
+      const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc]);
+      const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc + 2]);
+      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int64_t ci = n0 + tc + j;
+    if (ci >= g.ncols) continue;
+    const int64_t child0 = g.c0 + 8 * ci;
+    double *ccol;
+    if (g.split) ccol = g.part + ((int64_t)blockIdx.z * g.ncols + ci) * g.R;
+    else ccol = g.X + (g.up ? (int64_t)g.cparent[child0] : child0) * g.nt2;
+#pragma unroll
+    for (int i = 0; i < 4; i += 2) {
+      const int row = r0 + wr + 8 * i;  // wr, then wr + 16; even, R is even
+      if (row >= g.R) continue;
+      double2 *dst = reinterpret_cast<double2 *>(ccol + row);
+      double2 v = make_double2(acc[i][j], acc[i + 1][j]);
+      if (!g.up) {
+        const double2 o = *dst;
+        v.x += o.x;
+        v.y += o.y;
+      }
+      *dst = v;
+    }
+  }
+}
+
+// Split M2M: M[parent_i] = sum over octants o = 0..7, in that order, of part[o][i].
+__global__ void sum_octant_parts(const double *__restrict__ part, int64_t ncols, int R,
+                                 int64_t c0, const int32_t *__restrict__ cparent, int nt2,
+                                 double *__restrict__ X) {
+  const int64_t total = ncols * R;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ci = e / R;
+    const int row = (int)(e - ci * R);
+    double v = 0;
+#pragma unroll
+    for (int o = 0; o < 8; o++) v += part[(o * ncols + ci) * R + row];
+    X[(int64_t)cparent[c0 + 8 * ci] * nt2 + row] = v;
+  }
+}
+
+// Builds this tree's per-level operators for order P (levels 0 .. nlev-1 have
+// children).
+template <int P>
+int build_level_ops(tapas_b200_ctx *ctx, int &nlev, LevelFirstChild &lf) {
+  using S = Sizes<P>;
+  cudaStream_t s = ctx->stream;
+  nlev = 0;
+  for (int l = 0; l + 2 < (int)ctx->level_off.size() && l < kMaxLevels; l++) {
+    if (ctx->level_off[l + 2] <= ctx->level_off[l + 1]) break;
+    lf.c0[l] = ctx->level_off[l + 1];
+    nlev = l + 1;
+  }
+  if (nlev == 0) return TAPAS_B200_OK;
+  const size_t per = (size_t)(2 * S::NT) * (16 * S::NT);  // doubles per level, either op
+  TB_CUDA(ctx, ctx->op_m2m.ensure(per * nlev, s));
+  TB_CUDA(ctx, ctx->op_l2l.ensure(per * nlev, s));
+  build_translation_ops<P><<<dim3(nlev, 8, 2), 256, 0, s>>>(lf, ctx->cparent.p, ctx->ccen.p,
+                                                           ctx->op_m2m.p, ctx->op_l2l.p);
+  TB_LAUNCH_CHECK(ctx);
+  return TAPAS_B200_OK;
+}
+
+template <int P>
+int level_translate(tapas_b200_ctx *ctx, int l, const LevelFirstChild &lf, bool up) {
+  using S = Sizes<P>;
+  const int64_t ncols = (ctx->level_off[l + 2] - ctx->level_off[l + 1]) / 8;
+  if (ncols <= 0) return TAPAS_B200_OK;
+  const size_t per = (size_t)(2 * S::NT) * (16 * S::NT);
+  LevelGemm g;
+  g.At = (up ? ctx->op_m2m.p : ctx->op_l2l.p) + per * l;
+  g.R = up ? 2 * S::NT : 16 * S::NT;
+  g.K = up ? 16 * S::NT : 2 * S::NT;
+  g.nt2 = 2 * S::NT;
+  g.up = up ? 1 : 0;
+  g.c0 = lf.c0[l];
+  g.ncols = ncols;
+  g.cparent = ctx->cparent.p;
+  g.X = reinterpret_cast<double *>(up ? ctx->M.p : ctx->L.p);
+  g.part = nullptr;
+  dim3 grid((unsigned)((ncols + kGN - 1) / kGN), (unsigned)((g.R + kGM - 1) / kGM));
+  // A level too small to fill the GPU splits M2M's eight octant products
+  // over blocks and adds them afterwards in octant order.
+  g.split = (up && (int64_t)grid.x * grid.y < 2 * ctx->num_sms) ? 1 : 0;
+  if (g.split) {
+    TB_CUDA(ctx, ctx->op_part.ensure((size_t)8 * ncols * g.R, ctx->stream));
+    g.part = ctx->op_part.p;
+    grid.z = 8;
+  }
+  level_gemm<<<grid, kGThreads, 0, ctx->stream>>>(g);
+  TB_LAUNCH_CHECK(ctx);
+  if (g.split) {
+    sum_octant_parts<<<grid_for(ncols * g.R, 256), 256, 0, ctx->stream>>>(
+        g.part, ncols, g.R, g.c0, g.cparent, g.nt2, g.X);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  return TAPAS_B200_OK;
+}
+
 template <int P>
 int upward_P(tapas_b200_ctx *ctx) {
   using S = Sizes<P>;
@@ -442,13 +628,11 @@ int upward_P(tapas_b200_ctx *ctx) {
     }
   }
   PhaseTimer t(ctx, &ctx->timings.m2m);
-  for (int lev = ctx->max_depth - 1; lev >= 0; lev--) {
-    const int64_t a = ctx->level_off[lev], cnt = ctx->level_off[lev + 1] - a;
-    if (cnt <= 0) continue;
-    m2m_kernel<P><<<(unsigned)((cnt + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        a, cnt, ctx->cleaf.p, ctx->cnb.p, ctx->cchild.p, ctx->ccen.p, ctx->M.p);
-    TB_LAUNCH_CHECK(ctx);
-  }
+  int nlev = 0;
+  LevelFirstChild lf;
+  TB_TRY(build_level_ops<P>(ctx, nlev, lf));
+  ctx->level_ops_P = P;
+  for (int lev = nlev - 1; lev >= 0; lev--) TB_TRY(level_translate<P>(ctx, lev, lf, true));
   return TAPAS_B200_OK;
 }
 
@@ -473,13 +657,19 @@ int downward_P(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
   {
     PhaseTimer t(ctx, &ctx->timings.l2l);
-    for (int lev = 1; lev <= ctx->max_depth; lev++) {
-      const int64_t a = ctx->level_off[lev], cnt = ctx->level_off[lev + 1] - a;
-      if (cnt <= 0) continue;
-      l2l_kernel<P><<<(unsigned)((cnt + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-          a, cnt, ctx->cnb.p, ctx->cparent.p, ctx->ccen.p, ctx->L.p);
-      TB_LAUNCH_CHECK(ctx);
+    int nlev = 0;
+    LevelFirstChild lf;
+    if (ctx->level_ops_P != P) {  // the operators of the upward pass are reused
+      TB_TRY(build_level_ops<P>(ctx, nlev, lf));
+      ctx->level_ops_P = P;
+    } else {
+      for (int l = 0; l + 2 < (int)ctx->level_off.size() && l < kMaxLevels; l++) {
+        if (ctx->level_off[l + 2] <= ctx->level_off[l + 1]) break;
+        lf.c0[l] = ctx->level_off[l + 1];
+        nlev = l + 1;
+      }
     }
+    for (int lev = 0; lev < nlev; lev++) TB_TRY(level_translate<P>(ctx, lev, lf, false));
   }
   PhaseTimer t(ctx, &ctx->timings.l2p);
   const int64_t nl = ctx->n_nonempty_leaves;

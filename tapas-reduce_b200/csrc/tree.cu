@@ -276,6 +276,7 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
     return TAPAS_B200_ERR_ARG;
   }
   ctx->have_tree = ctx->have_lists = ctx->have_M = ctx->have_L = false;
+  ctx->level_ops_P = 0;  // translation operators belong to the previous tree
   ctx->ncrit = ncrit;
   TB_CUDA(ctx, ctx->keys.ensure(n, s));
   TB_CUDA(ctx, ctx->keys_alt.ensure(n, s));
