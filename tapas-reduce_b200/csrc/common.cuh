@@ -104,14 +104,14 @@ struct Mlp;  // learned-chooser network (mlp.cu)
 struct TcState {
   DBuf<uint64_t> keys, keys_alt, tc_keys;
   DBuf<uint32_t> vals, vals_alt;
-  DBuf<uint8_t> use64;
+  DBuf<uint32_t> pairs64;  // list indices of the pairs left to the FP64 kernel
   DBuf<int32_t> flag, scan, seg_start, tcflag, tcid, ntiles, tile_off;
   DBuf<int4> items;
   DBuf<float> ops_hi, ops_lo, Mt, Lt;
   DBuf<int> err;
   void release() {
     keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();
-    use64.release(); flag.release(); scan.release(); seg_start.release(); tcflag.release();
+    pairs64.release(); flag.release(); scan.release(); seg_start.release(); tcflag.release();
     tcid.release(); ntiles.release(); tile_off.release(); items.release(); ops_hi.release();
     ops_lo.release(); Mt.release(); Lt.release(); err.release();
   }
@@ -195,7 +195,8 @@ struct tapas_b200_ctx {
   int64_t p2p_nitems = 0;
   bool p2p_split = false;
   tb::TcState tc;                       // mixed: tensor-core M2L work state
-  const uint8_t *m2l_use = nullptr;     // FP64 M2L: evaluate only pairs with use[e] != 0
+  const uint32_t *m2l_pairs = nullptr;  // FP64 M2L of listed pairs: their list indices
+  int64_t m2l_npairs = 0;
   int64_t tc_classes = 0, tc_tiles = 0, tc_segments = 0, n_m2l_tc = 0;
   size_t tc_op_budget = (size_t)4 << 30;  // bytes of split-TF32 operators kept at once
   bool have_M = false, have_L = false;

@@ -83,15 +83,17 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
   for (int base = 0; base < nb; base += 32) {
     const int b = base + lane;
     const bool valid = b < nb;
-    double q = 0, rho = 1, alpha = 0, beta = 0;
+    double q = 0, dx = 0, dy = 0, dz = 0;
     if (valid) {
       q = sq[b0 + b];
-      cart2sph(sx[b0 + b] - cx, sy[b0 + b] - cy, sz[b0 + b] - cz, rho, alpha, beta);
+      dx = sx[b0 + b] - cx;
+      dy = sy[b0 + b] - cy;
+      dz = sz[b0 + b] - cz;
     }
-    const double x = cos(alpha), y = sin(alpha);
-    double sb, cb;
-    sincos(beta, &sb, &cb);
-    const cd ei{cb, sb};
+    // cart2sph (:43-47) then cos/sin of the angles, formed directly
+    const Sph sp = sph_of(dx, dy, dz);
+    const double rho = sp.r, x = sp.x, y = sp.y;
+    const cd ei = sp.ei;
     // Streamed evalMultipole (:63-99): this body's q*conj(Y_n^m) terms, 8 at a
     // time, summed over the warp's bodies by one reduce-scatter.
     double buf[16];
@@ -144,6 +146,33 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
 // ---------------------------------------------------------------------------
 // M2L (:208-273, mutual = 0): L[t] = sum over sources s of T(c_t - c_s) M[s]
 // ---------------------------------------------------------------------------
+// One source's translation added to lane coefficients (jj[r], kk[r]): the
+// source's M in Mj, the local harmonics of the offset in Y.
+template <int P>
+__device__ __forceinline__ void m2l_accumulate(cd (&acc)[Sizes<P>::R], const int (&jj)[Sizes<P>::R],
+                                               const int (&kk)[Sizes<P>::R], int lane,
+                                               const cd *Mj, const cd *Y) {
+  using S = Sizes<P>;
+#pragma unroll
+  for (int r = 0; r < S::R; r++) {
+    if (lane + 32 * r >= S::NT) continue;
+    const int j = jj[r], k = kk[r];
+    const double Cnm = oddeven(j);
+    for (int n = 0; n < P - j; n++) {
+      const int base = (j + n) * (j + n) + j + n - k;
+      for (int m = -n; m < 0; m++) {
+        const int nms = n * (n + 1) / 2 - m;
+        cmac(acc[r], scal(Cnm, conjd(Mj[nms])), Y[base + m]);
+      }
+      for (int m = 0; m <= n; m++) {
+        const int nms = n * (n + 1) / 2 + m;
+        const double Cnm2 = Cnm * oddeven((k - m) * (k < m) + m);
+        cmac(acc[r], scal(Cnm2, Mj[nms]), Y[base + m]);
+      }
+    }
+  }
+}
+
 template <int P>
 __global__ void __launch_bounds__(kThreads) m2l_kernel(
     int64_t ncells, const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
@@ -170,7 +199,7 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
   for (int e = e0; e < e1; e++) {
     const int s = (int)(list[e] & src_mask);
     if (cnb[s] == 0) continue;  // M of an empty cell is exactly zero
-    if (use && !use[e]) continue;  // pair evaluated elsewhere (tensor-core classes)
+    if (use && !use[e]) continue;  // optional pair mask (null: every pair)
     const Sph sp = sph_of(tx - ccen[3 * s], ty - ccen[3 * s + 1], tz - ccen[3 * s + 2]);
     __syncwarp();
     if (lane < P) local_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
@@ -202,6 +231,54 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
   for (int r = 0; r < S::R; r++) {
     const int t = lane + 32 * r;
     if (t < S::NT) L[c * S::NT + t] = make_double2(acc[r].x, acc[r].y);
+  }
+}
+
+// The mixed form's FP64 remainder: one warp per listed pair (list index),
+// added into L[target] with atomics, so a target with many such pairs does
+// not hold one warp alone.
+template <int P>
+__global__ void __launch_bounds__(kThreads) m2l_pair_kernel(
+    const uint32_t *__restrict__ pairs, int64_t npairs, const uint64_t *__restrict__ list,
+    int shift, const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
+    const double2 *__restrict__ M, double2 *__restrict__ L) {
+  using S = Sizes<P>;
+  __shared__ cd Ysm[kWarps][S::NY];
+  __shared__ cd Msm[kWarps][S::NT];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  cd *Y = Ysm[wi];
+  cd *Mj = Msm[wi];
+  int jj[S::R], kk[S::R];
+#pragma unroll
+  for (int r = 0; r < S::R; r++) jk_of(lane + 32 * r, jj[r], kk[r]);
+  const uint64_t src_mask = (1ull << shift) - 1;
+  const int64_t nw = (int64_t)gridDim.x * kWarps;
+  for (int64_t p = (int64_t)blockIdx.x * kWarps + wi; p < npairs; p += nw) {
+    const uint64_t x = list[pairs[p]];
+    const int c = (int)(x >> shift), s = (int)(x & src_mask);
+    if (cnb[s] == 0 || cnb[c] == 0) continue;
+    const Sph sp = sph_of(ccen[3 * c] - ccen[3 * s], ccen[3 * c + 1] - ccen[3 * s + 1],
+                          ccen[3 * c + 2] - ccen[3 * s + 2]);
+    __syncwarp();
+    if (lane < P) local_column<P>(lane, sp.r, sp.x, sp.y, sp.ei, Y);
+    for (int t = lane; t < S::NT; t += 32) {
+      double2 v = M[(int64_t)s * S::NT + t];
+      Mj[t] = cd{v.x, v.y};
+    }
+    __syncwarp();
+    cd acc[S::R];
+#pragma unroll
+    for (int r = 0; r < S::R; r++) acc[r] = cd{0, 0};
+    m2l_accumulate<P>(acc, jj, kk, lane, Mj, Y);
+    double *Lc = reinterpret_cast<double *>(L + (int64_t)c * S::NT);
+#pragma unroll
+    for (int r = 0; r < S::R; r++) {
+      const int t = lane + 32 * r;
+      if (t < S::NT) {
+        atomicAdd(Lc + 2 * t, acc[r].x);
+        atomicAdd(Lc + 2 * t + 1, acc[r].y);
+      }
+    }
   }
 }
 
@@ -647,8 +724,26 @@ int m2l_P(tapas_b200_ctx *ctx) {
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   m2l_kernel<P><<<(unsigned)((C + kWarps - 1) / kWarps), kThreads, 0, s>>>(
       C, ctx->m2l_off.p, ctx->m2l.p, mask, ctx->cnb.p, ctx->ccen.p, ctx->M.p, ctx->L.p,
-      ctx->m2l_use);
+      nullptr);
   TB_LAUNCH_CHECK(ctx);
+  return TAPAS_B200_OK;
+}
+
+template <int P>
+int m2l_pairs_P(tapas_b200_ctx *ctx) {
+  using S = Sizes<P>;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
+  TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
+  PhaseTimer t(ctx, &ctx->timings.m2l_fp64);
+  const int64_t np = ctx->m2l_npairs;
+  if (np > 0) {
+    m2l_pair_kernel<P><<<grid_for(np, kWarps, ctx->num_sms * 16), kThreads, 0, s>>>(
+        ctx->m2l_pairs, np, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->ccen.p, ctx->M.p,
+        ctx->L.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
   return TAPAS_B200_OK;
 }
 
@@ -697,17 +792,16 @@ int downward_P(tapas_b200_ctx *ctx) {
   return TAPAS_B200_ERR_UNSUPPORTED;
 
 int upward_fp64(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_P) }
-int m2l_fp64(tapas_b200_ctx *ctx) {
-  ctx->m2l_use = nullptr;
-  TB_DISPATCH_P(ctx->P, m2l_P)
-}
+int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
 
-static int m2l_fp64_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
+static int m2l_pairs_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_pairs_P) }
 
-int m2l_fp64_masked(tapas_b200_ctx *ctx, const uint8_t *use) {
-  ctx->m2l_use = use;
-  const int rc = m2l_fp64_dispatch(ctx);
-  ctx->m2l_use = nullptr;
+int m2l_fp64_pairs(tapas_b200_ctx *ctx, const uint32_t *pairs, int64_t npairs) {
+  ctx->m2l_pairs = pairs;
+  ctx->m2l_npairs = npairs;
+  const int rc = m2l_pairs_dispatch(ctx);
+  ctx->m2l_pairs = nullptr;
+  ctx->m2l_npairs = 0;
   return rc;
 }
 int downward_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, downward_P) }

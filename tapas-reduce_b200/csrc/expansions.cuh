@@ -35,7 +35,8 @@ struct RecipTable {
 static __constant__ RecipTable kRecip = RecipTable();
 __device__ __forceinline__ double recip(int i) { return kRecip.v[i]; }
 
-// cart2sph (ex/LaplaceSphericalCPU_tapas.h:43-47); used per body (P2M, L2P).
+// cart2sph (ex/LaplaceSphericalCPU_tapas.h:43-47); L2P takes the angles from
+// it (measured faster there than the direct form below).
 __device__ __forceinline__ void cart2sph(double dx, double dy, double dz, double &r,
                                          double &theta, double &phi) {
   r = sqrt(dx * dx + dy * dy + dz * dz);
@@ -43,7 +44,7 @@ __device__ __forceinline__ void cart2sph(double dx, double dy, double dz, double
   phi = atan2(dy, dx);
 }
 
-// What the translations (M2M, M2L, L2L) need of cart2sph: r, cos(theta),
+// What the other expansions need of cart2sph: r, cos(theta),
 // sin(theta) and e^{i phi}, formed directly from the offset instead of through
 // acos, atan2, cos and sin.  r = 0 gives theta = phi = 0 and an offset along
 // the z axis phi = 0, as there.

@@ -6,8 +6,9 @@ namespace tb {
 // FP64 expansion passes (expansions.cu); P in [kMinP, kMaxP].
 int upward_fp64(tapas_b200_ctx *ctx, int P);
 int m2l_fp64(tapas_b200_ctx *ctx);
-// FP64 M2L over the pairs e with use[e] != 0 only (L is zeroed first).
-int m2l_fp64_masked(tapas_b200_ctx *ctx, const uint8_t *use);
+// L zeroed, then the FP64 M2L of the pairs at list indices pairs[0..npairs)
+// added into it (atomics: the order of a target's sums is not fixed).
+int m2l_fp64_pairs(tapas_b200_ctx *ctx, const uint32_t *pairs, int64_t npairs);
 int downward_fp64(tapas_b200_ctx *ctx);
 // Near field (p2p.cu).
 int p2p_fp64(tapas_b200_ctx *ctx);

@@ -15,7 +15,8 @@
 //  1. classify: class key per M2L pair; stable radix sort of the pairs by key
 //     (the target order inside a class is kept); segments = classes.
 //  2. classes with >= kTcMin pairs run on the tensor cores; the rest (and
-//     pairs whose offset does not fit the key) stay on the FP64 kernel.
+//     pairs whose offset does not fit the key) are listed for the FP64
+//     kernel, which takes them one warp per pair.
 //  3. per tensor-core class the real K x K operator is built in FP64 from the
 //     unit-width singular harmonics and split into TF32 hi + lo parts, laid
 //     out as K-major core matrices (8 rows x 16 bytes) ready for smem.
@@ -196,18 +197,29 @@ __global__ void class_tc_flags(const int32_t *__restrict__ seg_start, int64_t ns
 }
 
 // Pairs of non-tensor-core classes (except empty-source pairs) go to FP64.
-__global__ void mark_fp64_pairs(const int32_t *__restrict__ seg_scan_incl_flag,
-                                const int32_t *__restrict__ scan, const int32_t *__restrict__ flag,
+// Appends the list index of every pair of a class left to FP64 to pairs64
+// (order set by the atomics; *n64 counts them).
+__global__ void mark_fp64_pairs(const int32_t *__restrict__ scan, const int32_t *__restrict__ flag,
                                 const int32_t *__restrict__ tcflag,
                                 const uint64_t *__restrict__ keys, KeyPack kp,
                                 const uint32_t *__restrict__ vals, int64_t n,
-                                uint8_t *__restrict__ use64) {
-  (void)seg_scan_incl_flag;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int cls = scan[i] + flag[i] - 1;  // inclusive scan - 1
-    const bool empty = keys[i] == kp.empty();
-    use64[vals[i]] = (!empty && !tcflag[cls]) ? 1 : 0;
+                                uint32_t *__restrict__ pairs64, int *__restrict__ n64) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    bool fp64 = false;
+    if (i < n) {
+      const int cls = scan[i] + flag[i] - 1;  // inclusive scan - 1
+      fp64 = keys[i] != kp.empty() && !tcflag[cls];
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, fp64);
+    if (mask) {
+      int b = 0;
+      if (lane == __ffs(mask) - 1) b = atomicAdd(n64, __popc(mask));
+      b = __shfl_sync(0xffffffffu, b, __ffs(mask) - 1);
+      if (fp64) pairs64[b + __popc(mask & ((1u << lane) - 1))] = vals[i];
+    }
   }
 }
 
@@ -789,7 +801,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_CUDA(ctx, T.keys_alt.ensure(n + 1, s));
   TB_CUDA(ctx, T.vals.ensure(n + 1, s));
   TB_CUDA(ctx, T.vals_alt.ensure(n + 1, s));
-  TB_CUDA(ctx, T.use64.ensure(n + 1, s));
+  TB_CUDA(ctx, T.pairs64.ensure(n + 1, s));
   if (n == 0) return TAPAS_B200_OK;
   // key width from the lists' largest offsets
   TB_CUDA(ctx, T.err.ensure(4, s));
@@ -866,14 +878,16 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(scan_exclusive(ctx, T.tcflag.p, T.tcid.p, nseg, T.tcid.p + nseg));
   TB_TRY(scan_exclusive(ctx, T.ntiles.p, T.tile_off.p, nseg, T.tile_off.p + nseg));
+  TB_CUDA(ctx, cudaMemsetAsync(T.err.p + 3, 0, sizeof(int), s));
   mark_fp64_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
-      nullptr, T.scan.p, T.flag.p, T.tcflag.p, T.keys.p, kp, T.vals.p, n, T.use64.p);
+      T.scan.p, T.flag.p, T.tcflag.p, T.keys.p, kp, T.vals.p, n, T.pairs64.p, T.err.p + 3);
   TB_LAUNCH_CHECK(ctx);
   TB_CUDA(ctx, cudaMemcpyAsync(h, T.tcid.p + nseg, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TB_CUDA(ctx, cudaMemcpyAsync(h + 1, T.tile_off.p + nseg, sizeof(int32_t),
                                cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaMemcpyAsync(h + 2, T.err.p + 3, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TB_CUDA(ctx, cudaStreamSynchronize(s));
-  const int64_t ntc = h[0], nitems = h[1];
+  const int64_t ntc = h[0], nitems = h[1], n64 = h[2];
   ctx->tc_classes = ntc;
   ctx->tc_tiles = nitems;
   ctx->tc_segments = nseg;
@@ -903,7 +917,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
   setup_timer.reset();
   // 5. FP64 part (rare classes) writes L; the GEMM adds into Lt
-  TB_TRY(m2l_fp64_masked(ctx, T.use64.p));
+  TB_TRY(m2l_fp64_pairs(ctx, T.pairs64.p, n64));
   if (nitems > 0) {
     PhaseTimer t(ctx, &ctx->timings.m2l_tc);
     const float *mt_hi = T.Mt.p, *mt_lo = T.Mt.p + (size_t)C * S::KP;
