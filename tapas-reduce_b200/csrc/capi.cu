@@ -184,6 +184,7 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->front_b.release();
   ctx->counters.release();
   ctx->trav_geo.release();
+  ctx->body_pack.release();
   ctx->trav_meta.release();
   ctx->list_src.release();
   ctx->M.release();

@@ -135,6 +135,7 @@ struct tapas_b200_ctx {
   // ---- bodies (SoA FP64) ----
   int64_t n = 0;
   tb::DBuf<double> x, y, z, q;          // input order
+  tb::DBuf<double4> body_pack;          // input order, (x, y, z, q) per body
   tb::DBuf<double> sx, sy, sz, sq;      // sorted order
   tb::DBuf<uint64_t> keys, keys_alt;    // sort ping-pong
   tb::DBuf<uint32_t> idx, idx_alt;      // sorted position -> original index

@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
                                                        float *__restrict__ ops_lo) {
   using S = TcShape<P>;
   __shared__ cd Y[P * P];
+  __shared__ double scale[P];                        // (w_s / w_t)^n = 2^(delta n)
+  __shared__ unsigned char deg[S::NT], ord[S::NT];   // (j, k) of coefficient t
   const int cls = blockIdx.x;
   const uint64_t key = tc_keys[cls];
   const int delta = (int)((key >> 42) & 63) - 32;
@@ -288,99 +290,136 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
   // offset in units of the target width: D * 2^(min(delta,0) - 1)
   const double u = ldexp(1.0, min(delta, 0) - 1);
   const Sph sp = sph_of(Dx * u, Dy * u, Dz * u);
-  if (threadIdx.x < P) local_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
+  if (threadIdx.x < P) {
+    local_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
+    scale[threadIdx.x] = ldexp(1.0, delta * (int)threadIdx.x);
+  }
+  for (int t = threadIdx.x; t < S::NT; t += blockDim.x) {
+    int j, k;
+    jk_of(t, j, k);
+    deg[t] = (unsigned char)j;
+    ord[t] = (unsigned char)k;
+  }
   __syncthreads();
   float *hi = ops_hi + (size_t)cls * S::MP * S::KP;
   float *lo = ops_lo + (size_t)cls * S::MP * S::KP;
-  for (int idx = threadIdx.x; idx < S::MP * S::KP; idx += blockDim.x) {
-    const int r = idx / S::KP, c = idx % S::KP;
-    double val = 0;
-    if (r < S::K && c < S::K) {
-      const int to = r >> 1, ti = c >> 1;  // complex output / input coefficient
-      const bool rim = r & 1, cim = c & 1;
-      int j, k, n, ma;
-      jk_of(to, j, k);
-      jk_of(ti, n, ma);
+  // one thread per complex (output, input) pair: its real 2 x 2 block
+  for (int idx = threadIdx.x; idx < (S::MP / 2) * (S::KP / 2); idx += blockDim.x) {
+    const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // complex output / input
+    double v00 = 0, v01 = 0, v10 = 0, v11 = 0;  // [row re/im][column re/im]
+    if (2 * to < S::K && 2 * ti < S::K) {
+      const int j = deg[to], k = ord[to], n = deg[ti], ma = ord[ti];
       if (n < P - j) {
         const double Cnm = oddeven(j);
         const int base = (j + n) * (j + n) + j + n - k;
         // m = +ma term: M * Cnm2 * Y[j+n, ma-k]
-        {
-          const double C2 = Cnm * oddeven((k - ma) * (k < ma) + ma);
-          const cd Yv = Y[base + ma];
-          const double cc = Yv.x, dd = Yv.y;
-          if (!rim && !cim) val += C2 * cc;
-          else if (!rim && cim) val += -C2 * dd;
-          else if (rim && !cim) val += C2 * dd;
-          else val += C2 * cc;
-        }
+        const double C2 = Cnm * oddeven((k - ma) * (k < ma) + ma);
+        const cd Yp = Y[base + ma];
+        v00 = C2 * Yp.x;
+        v01 = -C2 * Yp.y;
+        v10 = C2 * Yp.y;
+        v11 = C2 * Yp.x;
         // m = -ma term (ma > 0): conj(M) * Cnm * Y[j+n, -ma-k]
         if (ma > 0) {
-          const cd Yv = Y[base - ma];
-          const double cc = Yv.x, dd = Yv.y;
-          if (!rim && !cim) val += Cnm * cc;
-          else if (!rim && cim) val += Cnm * dd;
-          else if (rim && !cim) val += Cnm * dd;
-          else val += -Cnm * cc;
+          const cd Ym = Y[base - ma];
+          v00 += Cnm * Ym.x;
+          v01 += Cnm * Ym.y;
+          v10 += Cnm * Ym.y;
+          v11 += -Cnm * Ym.x;
         }
-        val = ldexp(val, delta * n);  // (w_s / w_t)^n
+        const double sc = scale[n];  // exact: a power of two in the normal range
+        v00 *= sc; v01 *= sc; v10 *= sc; v11 *= sc;
       }
     }
-    const float f = (float)val;
-    const float h = tf32_round(f);
-    const float l = tf32_round(f - h);
-    const size_t o = op_offset<P>(r, c);
-    hi[o] = h;
-    lo[o] = l;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// normalised FP32 multipoles and the final rescale into FP64 L
-// ---------------------------------------------------------------------------
-// Mt_hi + Mt_lo = the normalised multipole M_n / w^n as split TF32 (the GEMM's
-// B operand, one row of KP values per cell).
-template <int P>
-__global__ void normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
-                            const double *__restrict__ cmin, const double *__restrict__ cmax,
-                            const double2 *__restrict__ M, float *__restrict__ Mt_hi,
-                            float *__restrict__ Mt_lo) {
-  using S = TcShape<P>;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells * S::KP;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = i / S::KP;
-    const int kk = (int)(i % S::KP);
-    float v = 0.f;
-    if (kk < S::K && cnb[c] > 0) {
-      int n, m;
-      jk_of(kk >> 1, n, m);
-      const double w = cmax[3 * c] - cmin[3 * c];
-      const double2 z = M[c * S::NT + (kk >> 1)];
-      v = (float)(((kk & 1) ? z.y : z.x) * pow(w, -n));
+    const double v[4] = {v00, v01, v10, v11};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float f = (float)v[e];
+      const float h = tf32_round(f);
+      const size_t o = op_offset<P>(2 * to + (e >> 1), 2 * ti + (e & 1));
+      hi[o] = h;
+      lo[o] = tf32_round(f - h);
     }
-    const float h = tf32_round(v);
-    Mt_hi[i] = h;
-    Mt_lo[i] = tf32_round(v - h);
   }
 }
 
+// Per cell c (one warp each): Mt[c][2t + (0: re, 1: im)] = M[c][t] / w^n
+// (n = degree of t, w = the cell's width), split into TF32 hi + lo.
 template <int P>
-__global__ void add_scaled_L(int64_t ncells, const int32_t *__restrict__ cnb,
-                             const double *__restrict__ cmin, const double *__restrict__ cmax,
-                             const float *__restrict__ Lt, double2 *__restrict__ L) {
+__global__ void __launch_bounds__(256) normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
+                                                   const double *__restrict__ cmin,
+                                                   const double *__restrict__ cmax,
+                                                   const double2 *__restrict__ M,
+                                                   float *__restrict__ Mt_hi,
+                                                   float *__restrict__ Mt_lo) {
   using S = TcShape<P>;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncells * S::NT;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = i / S::NT;
-    const int t = (int)(i % S::NT);
-    if (cnb[c] == 0) continue;
-    int j, k;
-    jk_of(t, j, k);
-    const double w = cmax[3 * c] - cmin[3 * c];
-    const double sc = pow(w, -(j + 1));
-    const double2 o = L[i];
-    L[i] = make_double2(o.x + (double)Lt[c * S::KP + 2 * t] * sc,
-                        o.y + (double)Lt[c * S::KP + 2 * t + 1] * sc);
+  constexpr int kSlots = (S::KP + 31) / 32;
+  __shared__ double pw[8][P];  // per warp: w^-n
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  int deg[kSlots];
+#pragma unroll
+  for (int r = 0; r < kSlots; r++) {
+    const int kk = lane + 32 * r;
+    int j = 0, k;
+    if (kk < S::K) jk_of(kk >> 1, j, k);
+    deg[r] = j;
+  }
+  const int64_t nw = (int64_t)gridDim.x * 8;
+  for (int64_t c = (int64_t)blockIdx.x * 8 + wi; c < ncells; c += nw) {
+    const bool live = cnb[c] > 0;
+    __syncwarp();
+    if (live && lane < P) pw[wi][lane] = pow(cmax[3 * c] - cmin[3 * c], -lane);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kSlots; r++) {
+      const int kk = lane + 32 * r;
+      if (kk >= S::KP) continue;
+      float v = 0.f;
+      if (live && kk < S::K) {
+        const double2 z = M[c * S::NT + (kk >> 1)];
+        v = (float)(((kk & 1) ? z.y : z.x) * pw[wi][deg[r]]);
+      }
+      const float h = tf32_round(v);
+      Mt_hi[c * S::KP + kk] = h;
+      Mt_lo[c * S::KP + kk] = tf32_round(v - h);
+    }
+  }
+}
+
+// Per cell c (one warp each): L[c][t] += Lt[c][t] / w^(j+1) (j = degree of t).
+template <int P>
+__global__ void __launch_bounds__(256) add_scaled_L(int64_t ncells, const int32_t *__restrict__ cnb,
+                                                    const double *__restrict__ cmin,
+                                                    const double *__restrict__ cmax,
+                                                    const float *__restrict__ Lt,
+                                                    double2 *__restrict__ L) {
+  using S = TcShape<P>;
+  constexpr int kSlots = (S::NT + 31) / 32;
+  __shared__ double pw[8][P + 1];  // per warp: w^-n, n = 0..P
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  int deg[kSlots];
+#pragma unroll
+  for (int r = 0; r < kSlots; r++) {
+    const int t = lane + 32 * r;
+    int j = 0, k;
+    if (t < S::NT) jk_of(t, j, k);
+    deg[r] = j;
+  }
+  const int64_t nw = (int64_t)gridDim.x * 8;
+  for (int64_t c = (int64_t)blockIdx.x * 8 + wi; c < ncells; c += nw) {
+    if (cnb[c] == 0) continue;  // warp-uniform
+    __syncwarp();
+    if (lane <= P) pw[wi][lane] = pow(cmax[3 * c] - cmin[3 * c], -lane);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kSlots; r++) {
+      const int t = lane + 32 * r;
+      if (t >= S::NT) continue;
+      const double sc = pw[wi][deg[r] + 1];
+      const float2 lt = *reinterpret_cast<const float2 *>(Lt + c * S::KP + 2 * t);
+      const double2 o = L[c * S::NT + t];
+      L[c * S::NT + t] = make_double2(o.x + (double)lt.x * sc, o.y + (double)lt.y * sc);
+    }
   }
 }
 
@@ -911,7 +950,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   // 4. normalised multipoles, zeroed normalised locals
   TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));  // hi rows, then lo rows
   TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
-  normalize_M<P><<<grid_for(C * S::KP, 256, ctx->num_sms * 32), 256, 0, s>>>(
+  normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
       C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP);
   TB_LAUNCH_CHECK(ctx);
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
@@ -931,7 +970,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
                                                         mt_hi, mt_lo, T.Lt.p, T.err.p);
     TB_LAUNCH_CHECK(ctx);
   }
-  add_scaled_L<P><<<grid_for(C * S::NT, 256, ctx->num_sms * 32), 256, 0, s>>>(
+  add_scaled_L<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
       C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, T.Lt.p, ctx->L.p);
   TB_LAUNCH_CHECK(ctx);
   TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -24,9 +24,12 @@
 // and the FP64 centre difference, so the separation x_i - x_j is formed from
 // ~47-bit operands and rounds once.  1/r is the hardware rsqrt (its error is far below
 // the near field's summation error, so no Newton step).
-// A source leaf whose box lies at least one target-leaf width away from the
-// target's box (every pair at least that far apart) skips the lo parts: one
-// rounding of a coordinate is then <= ~2e-7 of the separation.
+// A source leaf whose box is far enough from the target's box skips the lo
+// parts.  In the target frame a source coordinate is at most gap + tw/2 + sw
+// in magnitude (gap: the boxes' separation along the farthest axis, tw, sw:
+// the target and source widths) and every separation is at least gap, so one
+// rounding of a coordinate is at most 2^-24 (gap + tw/2 + sw) / gap of the
+// separation; with gap >= (tw/2 + sw) / 2 that is <= 3 * 2^-24 ~ 1.8e-7.
 // Each source leaf is summed in plain FP32 and the partial is Kahan-added into
 // the target's (sum, compensation) pair; the final near field is FP64.
 #include <algorithm>
@@ -331,7 +334,7 @@ struct __align__(16) SrcRec {
 // target leaf (FP64 difference as FP32 hi + lo).
 struct __align__(16) LeafMeta {
   int b0, ns;
-  int far;  // the leaf's box is at least one target-leaf width from the target's
+  int far;  // the leaf's box is far enough for plain FP32 coordinates (see above)
   float hx, hy, hz, lx, ly, lz;
 };
 
@@ -384,10 +387,10 @@ __device__ __forceinline__ void mixed_tile(
                    dcz = ccen[3 * s + 2] - tcz;
       m.hx = (float)dcx; m.hy = (float)dcy; m.hz = (float)dcz;
       m.lx = (float)(dcx - m.hx); m.ly = (float)(dcy - m.hy); m.lz = (float)(dcz - m.hz);
-      // boxes separated by >= tw along some axis: every pair is >= tw apart
-      const double half = 0.5 * (tw + (cmax[3 * s] - cmin[3 * s]));
-      const double gap = fmax(fabs(dcx), fmax(fabs(dcy), fabs(dcz))) - half;
-      m.far = gap >= tw ? 1 : 0;
+      // boxes separated by gap along the farthest axis: every pair is >= gap apart
+      const double sw = cmax[3 * s] - cmin[3 * s];
+      const double gap = fmax(fabs(dcx), fmax(fabs(dcy), fabs(dcz))) - 0.5 * (tw + sw);
+      m.far = gap >= 0.5 * (0.5 * tw + sw) ? 1 : 0;
       meta[lane] = m;
     }
     __syncwarp();
@@ -439,8 +442,8 @@ __device__ __forceinline__ void mixed_tile(
         }
       }
       if (far) {
-        // separations >= the target leaf's width: plain FP32 coordinates in the
-        // target frame (relative error of a separation <= ~2e-7), no r = 0 case
+        // separated leaves: plain FP32 coordinates in the target frame (relative
+        // error of a separation <= ~1.8e-7), no r = 0 case
 #pragma unroll 2
         for (int k = gs; k < cnt; k += G) {
           const float4 bh = ss[wi][k].hi;

@@ -78,12 +78,16 @@ __global__ void bbox_final(const double *__restrict__ part, int nparts, double *
   }
 }
 
+// Keys of the bodies, and each body packed as one 32-byte record (x, y, z, q)
+// so the gather into key order reads one sector per body.
 __global__ void __launch_bounds__(kBlock) keys_kernel(const double *__restrict__ x,
                                                       const double *__restrict__ y,
-                                                      const double *__restrict__ z, int64_t n,
+                                                      const double *__restrict__ z,
+                                                      const double *__restrict__ q, int64_t n,
                                                       const double *__restrict__ box,
                                                       uint64_t *__restrict__ keys,
-                                                      uint32_t *__restrict__ idx) {
+                                                      uint32_t *__restrict__ idx,
+                                                      double4 *__restrict__ packed) {
   const double lo = box[0], hi = box[1];
   const int nfc = 1 << kMaxDepth;
   const double pitch = ddiv(dsub(hi, lo), (double)nfc);
@@ -99,21 +103,21 @@ __global__ void __launch_bounds__(kBlock) keys_kernel(const double *__restrict__
     }
     keys[i] = finest_key(a[0], a[1], a[2]);
     idx[i] = (uint32_t)i;
+    packed[i] = make_double4(p[0], p[1], p[2], q[i]);
   }
 }
 
 __global__ void __launch_bounds__(kBlock) gather_bodies(
-    const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
-    const double *__restrict__ q, const uint32_t *__restrict__ idx, int64_t n,
+    const double4 *__restrict__ packed, const uint32_t *__restrict__ idx, int64_t n,
     double *__restrict__ sx, double *__restrict__ sy, double *__restrict__ sz,
     double *__restrict__ sq) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t j = idx[i];
-    sx[i] = x[j];
-    sy[i] = y[j];
-    sz[i] = z[j];
-    sq[i] = q[j];
+    const double4 b = packed[idx[i]];
+    sx[i] = b.x;
+    sy[i] = b.y;
+    sz[i] = b.z;
+    sq[i] = b.w;
   }
 }
 
@@ -286,6 +290,7 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
   TB_CUDA(ctx, ctx->sy.ensure(n, s));
   TB_CUDA(ctx, ctx->sz.ensure(n, s));
   TB_CUDA(ctx, ctx->sq.ensure(n, s));
+  TB_CUDA(ctx, ctx->body_pack.ensure(n, s));
   TB_CUDA(ctx, ctx->trg.ensure(4 * n, s));
   TB_CUDA(ctx, ctx->bbox.ensure(2, s));
 
@@ -298,7 +303,8 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
     bbox_final<<<1, 32, 0, s>>>(ctx->scratch_d.p, nparts, ctx->bbox.p);
     TB_LAUNCH_CHECK(ctx);
     keys_kernel<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-        ctx->x.p, ctx->y.p, ctx->z.p, n, ctx->bbox.p, ctx->keys.p, ctx->idx.p);
+        ctx->x.p, ctx->y.p, ctx->z.p, ctx->q.p, n, ctx->bbox.p, ctx->keys.p, ctx->idx.p,
+        ctx->body_pack.p);
     TB_LAUNCH_CHECK(ctx);
   }
   {
@@ -310,8 +316,7 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
     if (k != ctx->keys.p) { std::swap(ctx->keys.p, ctx->keys_alt.p); std::swap(ctx->keys.cap, ctx->keys_alt.cap); }
     if (v != ctx->idx.p) { std::swap(ctx->idx.p, ctx->idx_alt.p); std::swap(ctx->idx.cap, ctx->idx_alt.cap); }
     gather_bodies<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-        ctx->x.p, ctx->y.p, ctx->z.p, ctx->q.p, ctx->idx.p, n, ctx->sx.p, ctx->sy.p, ctx->sz.p,
-        ctx->sq.p);
+        ctx->body_pack.p, ctx->idx.p, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p);
     TB_LAUNCH_CHECK(ctx);
   }
   PhaseTimer t(ctx, &ctx->timings.tree);
