@@ -52,7 +52,9 @@ struct TcShape {
   static constexpr int K = 2 * NT;                    // real dimension
   static constexpr int MT = (K + 127) / 128;          // M-tiles of 128 operator rows
   static constexpr int MP = MT * 128;
-  static constexpr int KC = MT <= 2 ? 32 : 16;        // K chunk per stage
+  // K chunk per stage: small enough that the ring holds 4-6 stages (the
+  // copies of a stage take longer than its MMAs)
+  static constexpr int KC = MT <= 2 ? 16 : 8;
   static constexpr int KP = ((K + KC - 1) / KC) * KC; // padded K
   static constexpr int NKC = KP / KC;
   // TMEM accumulators: two (double-buffered epilogue) when they fit in the
@@ -62,12 +64,30 @@ struct TcShape {
   // one stage: A hi/lo (MP x KC) + B hi/lo (128 x KC) floats
   static constexpr int STAGE_FLOATS = 2 * MP * KC + 2 * kNTile * KC;
   // stages of the copy ring: as many as ~220 KB of shared memory holds (at
-  // most 4), and at most NKC + 1, so the copies run at most one tile ahead
+  // most 6), and at most NKC + 1, so the copies run at most one tile ahead
   static constexpr int NS_SMEM = (220 * 1024) / (STAGE_FLOATS * (int)sizeof(float));
-  static constexpr int NS_CAP = NS_SMEM < 4 ? NS_SMEM : 4;
+  static constexpr int NS_CAP = NS_SMEM < 6 ? NS_SMEM : 6;
   static constexpr int NS = NS_CAP < NKC + 1 ? NS_CAP : NKC + 1;
   static_assert(NS >= 2, "the copy ring needs two stages");
   static constexpr size_t SMEM = (size_t)NS * STAGE_FLOATS * sizeof(float) + 1024;
+  // An output row of degree j reads only sources of degree n < P - j, so
+  // M-tile mt (rows of degree >= jmin(mt)) has nonzero operator entries in
+  // its first kc_need(mt) K-chunks only; chunk kc is read by the first
+  // mcount(kc) M-tiles (kc_need falls with mt).
+  static constexpr int jmin(int mt) {
+    int j = 0;
+    while ((j + 1) * (j + 2) / 2 <= 64 * mt) j++;
+    return j;
+  }
+  static constexpr int kc_need(int mt) {
+    const int c = ((P - jmin(mt)) * (P - jmin(mt) + 1) + KC - 1) / KC;
+    return c < NKC ? c : NKC;
+  }
+  static constexpr int mcount(int kc) {
+    int m = 0;
+    for (int mt = 0; mt < MT; mt++) m += kc_need(mt) > kc ? 1 : 0;
+    return m;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -559,6 +579,7 @@ template <int P>
 __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, uint32_t a_lo,
                                                  uint32_t b_hi, uint32_t b_lo, int kc) {
   using S = TcShape<P>;
+  const int mcnt = S::mcount(kc);  // M-tiles with nonzero operator entries in this chunk
   // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
                          ((uint32_t)(128 >> 4) << 24);
@@ -566,6 +587,7 @@ __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, u
   const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
 #pragma unroll
   for (int mt = 0; mt < S::MT; mt++) {
+    if (mt >= mcnt) break;
     const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
     const uint32_t d = dcol + (uint32_t)(mt * kNTile);
 #pragma unroll
@@ -660,15 +682,19 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
 
   if (warp < kEpiWarp0) {
     // ---------------- producers ----------------
-    // B: each row chunk is KC floats = PPR 16-byte pieces; PPR consecutive
-    // lanes copy one row's chunk, so a warp instruction reads whole 128-byte
-    // (or 64-byte) row segments.  Thread t copies piece t % PPR of rows
-    // t / PPR + i * RPP (RPP = rows per pass of all producers, i < NRT) and
-    // fetches their sources and the tile's class one tile ahead.
+    // B: each row chunk is KC floats = PPR 16-byte pieces.  A warp copies 8
+    // rows x PPR pieces (PPR <= 4): lane l takes row l % 8 of the warp's
+    // group and piece l / 8, so its shared-memory writes fill whole core
+    // matrices (8 rows x 16 bytes, no bank conflicts) and each row's chunk is
+    // read as PPR x 16 contiguous bytes.  Thread t copies rows brow0 + i * RPP
+    // (RPP = rows per pass of all producers, i < NRT) and fetches their
+    // sources and the tile's class one tile ahead.
     constexpr int PPR = S::KC / 4;
-    constexpr int RPP = kProdThreads / PPR;
+    static_assert(PPR <= 4, "a warp covers 8 rows x PPR pieces");
+    constexpr int RPW = 32 / PPR;  // rows per warp instruction
+    constexpr int RPP = (kProdThreads / 32) * RPW;
     constexpr int NRT = kNTile / RPP;
-    const int bpiece = tid % PPR, brow0 = tid / PPR;
+    const int bpiece = (tid & 31) / RPW, brow0 = (tid >> 5) * RPW + (tid & 31) % RPW;
     int cur_src[NRT], nxt_src[NRT];
     int cur_cls = 0, nxt_cls = 0;
     auto fetch = [&](int64_t jt) {
@@ -697,7 +723,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
 #pragma unroll
         for (int i = 0; i < NRT; i++) cur_src[i] = nxt_src[i];
         cur_cls = nxt_cls;
-        fetch(jt + 1);
       }
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sA_lo = sA_hi + S::MP * S::KC;
@@ -705,7 +730,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       float *sB_lo = sB_hi + kNTile * S::KC;
       if (tid == 0) {
         const size_t aoff = (size_t)cur_cls * S::MP * S::KP + (size_t)kc * S::MP * S::KC;
-        const uint32_t abytes = (uint32_t)(S::MP * S::KC * sizeof(float));
+        // the chunk's rows of the M-tiles that read it: a prefix of its block
+        const uint32_t abytes = (uint32_t)(S::mcount(kc) * 128 * S::KC * sizeof(float));
         mbar_expect_tx(&full[st], 2 * abytes);
         bulk_copy(sA_hi, ops_hi + aoff, abytes, &full[st]);
         bulk_copy(sA_lo, ops_lo + aoff, abytes, &full[st]);
@@ -722,6 +748,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       }
       cp_async_arrive_noinc(&full[st]);
       issued = step + 1;
+      // the next tile's sources (a chain of dependent loads), after this
+      // tile's first copies are on their way
+      if (kc == 0) fetch(jt + 1);
     }
     cp_async_wait_all();
     if (tid == 0 && *abort) {
