@@ -382,6 +382,111 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
   }
 }
 
+// L2P of the mixed form in FP32: the local expansion's terms fall off
+// geometrically inside the leaf, so one FP32 evaluation of them is accurate
+// to ~1e-7 of the far-field potential; the result is added into the FP64
+// totals.
+template <int P>
+__global__ void __launch_bounds__(kThreads) l2p32_kernel(
+    const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
+    const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
+    const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
+    const double *__restrict__ sq, const double2 *__restrict__ L, double *__restrict__ trg,
+    int near_has_q) {
+  using S = Sizes<P>;
+  __shared__ float2 Lsm[kWarps][S::NT];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + wi;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int b0 = cbeg[c], nb = cnb[c];
+  float2 *Lc = Lsm[wi];
+  for (int t = lane; t < S::NT; t += 32) {
+    const double2 v = L[(int64_t)c * S::NT + t];
+    Lc[t] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncwarp();
+  const double cx = ccen[3 * c], cy = ccen[3 * c + 1], cz = ccen[3 * c + 2];
+  for (int b = lane; b < nb; b += 32) {
+    const int64_t bi = b0 + b;
+    const float dx = (float)(sx[bi] - cx), dy = (float)(sy[bi] - cy), dz = (float)(sz[bi] - cz);
+    // cart2sph (:43-47): r, cos/sin of theta and e^{i phi} from the offset
+    const float rxy2 = dx * dx + dy * dy;
+    const float r = sqrtf(rxy2 + dz * dz);
+    float x = 1.f, y = 0.f, cp = 1.f, sp = 0.f;
+    if (r > 0.f) {
+      const float rxy = sqrtf(rxy2);
+      x = dz / r;
+      y = rxy / r;
+      if (rxy > 0.f) {
+        cp = dx / rxy;
+        sp = dy / rxy;
+      }
+    }
+    const float inv_y = 1.f / y, inv_r = 1.f / r;
+    float pot = 0, s0 = 0, s1 = 0, s2 = 0;
+    float fact = 1, pn = 1, rhom = 1;
+    float2 eim = make_float2(1.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < P; m++) {
+      float p = pn, p1 = pn;
+      float rhon = rhom;
+      float2 sa = make_float2(0.f, 0.f), sb = sa, sc = sa;
+#pragma unroll
+      for (int n = m; n < P; n++) {
+        float ys, yt;
+        const float t1 = x * p1;
+        if (n == m) {
+          const float pnew = (float)(2 * m + 1) * t1;
+          ys = rhom * p;
+          yt = rhom * (pnew - (float)(m + 1) * t1);
+          p = pnew;
+          rhon = rhom * r;
+        } else {
+          rhon *= 1.f / (float)(-(n + m));  // constants after unrolling
+          ys = rhon * p;
+          const float p2 = p1;
+          p1 = p;
+          const float tn = x * p1;
+          p = ((float)(2 * n + 1) * tn - (float)(n + m) * p2) * (1.f / (float)(n - m + 1));
+          yt = rhon * ((float)(n - m + 1) * p - (float)(n + 1) * tn);
+          rhon *= r;
+        }
+        const float2 Lv = Lc[n * (n + 1) / 2 + m];
+        sa.x = fmaf(ys, Lv.x, sa.x);
+        sa.y = fmaf(ys, Lv.y, sa.y);
+        const float nys = (float)n * ys;
+        sb.x = fmaf(nys, Lv.x, sb.x);
+        sb.y = fmaf(nys, Lv.y, sb.y);
+        sc.x = fmaf(yt, Lv.x, sc.x);
+        sc.y = fmaf(yt, Lv.y, sc.y);
+      }
+      const float f = (m == 0) ? 1.f : 2.f;
+      const float zax = sa.x * eim.x - sa.y * eim.y, zay = sa.x * eim.y + sa.y * eim.x;
+      pot += f * zax;
+      s0 += f * inv_r * (sb.x * eim.x - sb.y * eim.y);
+      s1 += f * inv_y * (sc.x * eim.x - sc.y * eim.y);
+      if (m > 0) s2 += 2.f * (-zay) * (float)m;  // real(L*Y*i) = -imag(L*Y)
+      rhom = rhom * r * (1.f / (float)(-(2 * m + 2) * (2 * m + 1)));
+      pn = -pn * fact * y;
+      fact += 2.f;
+      eim = make_float2(eim.x * cp - eim.y * sp, eim.x * sp + eim.y * cp);
+    }
+    const float st = y, ct = x;
+    const float c0 = st * cp * s0 + ct * cp * inv_r * s1 - sp * inv_r * inv_y * s2;
+    const float c1 = st * sp * s0 + ct * sp * inv_r * s1 + cp * inv_r * inv_y * s2;
+    const float c2 = ct * s0 - st * inv_r * s1;
+    double *o = trg + 4 * bi;
+    // an FP64 near field holds q_i * sum(q_j / r) (the reference's TRG before
+    // its `ba /= b.SRC`)
+    const double iq = near_has_q ? 1.0 / sq[bi] : 1.0;
+    o[0] = o[0] * iq + (double)pot;
+    o[1] = o[1] * iq + (double)c0;
+    o[2] = o[2] * iq + (double)c1;
+    o[3] = o[3] * iq + (double)c2;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Level-batched M2M and L2L.
 //
@@ -748,7 +853,7 @@ int m2l_pairs_P(tapas_b200_ctx *ctx) {
 }
 
 template <int P>
-int downward_P(tapas_b200_ctx *ctx) {
+int downward_P(tapas_b200_ctx *ctx, bool l2p_f32) {
   cudaStream_t s = ctx->stream;
   {
     PhaseTimer t(ctx, &ctx->timings.l2l);
@@ -768,7 +873,13 @@ int downward_P(tapas_b200_ctx *ctx) {
   }
   PhaseTimer t(ctx, &ctx->timings.l2p);
   const int64_t nl = ctx->n_nonempty_leaves;
-  if (nl > 0) {
+  if (nl > 0 && l2p_f32) {
+    l2p32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+        ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
+        ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p,
+        ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
+    TB_LAUNCH_CHECK(ctx);
+  } else if (nl > 0) {
     l2p_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
         ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
         ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p, ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
@@ -804,6 +915,11 @@ int m2l_fp64_pairs(tapas_b200_ctx *ctx, const uint32_t *pairs, int64_t npairs) {
   ctx->m2l_npairs = 0;
   return rc;
 }
-int downward_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, downward_P) }
+template <int P>
+int downward_fp64_P(tapas_b200_ctx *ctx) { return downward_P<P>(ctx, false); }
+template <int P>
+int downward_f32leaf_P(tapas_b200_ctx *ctx) { return downward_P<P>(ctx, true); }
+int downward_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, downward_fp64_P) }
+int downward_fp32_l2p(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, downward_f32leaf_P) }
 
 }  // namespace tb

@@ -10,6 +10,8 @@ int m2l_fp64(tapas_b200_ctx *ctx);
 // added into it (atomics: the order of a target's sums is not fixed).
 int m2l_fp64_pairs(tapas_b200_ctx *ctx, const uint32_t *pairs, int64_t npairs);
 int downward_fp64(tapas_b200_ctx *ctx);
+// FP64 L2L, then L2P in FP32 added to the near field.
+int downward_fp32_l2p(tapas_b200_ctx *ctx);
 // Near field (p2p.cu).
 int p2p_fp64(tapas_b200_ctx *ctx);
 int p2p_mixed(tapas_b200_ctx *ctx);

@@ -1,9 +1,9 @@
 // Mixed-precision evaluation path (TAPAS_B200_MIXED).
 //
 // Near field: FP32 compensated P2P (p2p.cu, p2p_mixed).  M2L: offset-class
-// batched split-TF32 GEMMs on the tensor cores (m2l_tc.cu).  Upward and
-// downward passes stay FP64; the near-field result is per unit charge, so
-// L2P adds to it without the reference's division by q_i.
+// batched split-TF32 GEMMs on the tensor cores (m2l_tc.cu).  Upward pass and
+// L2L stay FP64; L2P runs in FP32 and adds to the near-field result, which is
+// per unit charge (so without the reference's division by q_i).
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
 #include "mixed.cuh"
@@ -14,7 +14,7 @@ int upward_mixed(tapas_b200_ctx *ctx, int P) { return upward_fp64(ctx, P); }
 
 int m2l_mixed(tapas_b200_ctx *ctx) { return m2l_tensorcore(ctx); }
 
-int downward_mixed(tapas_b200_ctx *ctx) { return downward_fp64(ctx); }
+int downward_mixed(tapas_b200_ctx *ctx) { return downward_fp32_l2p(ctx); }
 
 int mixed_sync_fp64_view(tapas_b200_ctx *ctx) {
   (void)ctx;

@@ -29,7 +29,7 @@
 // in magnitude (gap: the boxes' separation along the farthest axis, tw, sw:
 // the target and source widths) and every separation is at least gap, so one
 // rounding of a coordinate is at most 2^-24 (gap + tw/2 + sw) / gap of the
-// separation; with gap >= (tw/2 + sw) / 2 that is <= 3 * 2^-24 ~ 1.8e-7.
+// separation; with gap >= (tw/2 + sw) / 3 that is <= 4 * 2^-24 ~ 2.4e-7.
 // Each source leaf is summed in plain FP32 and the partial is Kahan-added into
 // the target's (sum, compensation) pair; the final near field is FP64.
 #include <algorithm>
@@ -390,7 +390,7 @@ __device__ __forceinline__ void mixed_tile(
       // boxes separated by gap along the farthest axis: every pair is >= gap apart
       const double sw = cmax[3 * s] - cmin[3 * s];
       const double gap = fmax(fabs(dcx), fmax(fabs(dcy), fabs(dcz))) - 0.5 * (tw + sw);
-      m.far = gap >= 0.5 * (0.5 * tw + sw) ? 1 : 0;
+      m.far = 3.0 * gap >= 0.5 * tw + sw ? 1 : 0;
       meta[lane] = m;
     }
     __syncwarp();
@@ -443,7 +443,7 @@ __device__ __forceinline__ void mixed_tile(
       }
       if (far) {
         // separated leaves: plain FP32 coordinates in the target frame (relative
-        // error of a separation <= ~1.8e-7), no r = 0 case
+        // error of a separation <= ~2.4e-7), no r = 0 case
 #pragma unroll 2
         for (int k = gs; k < cnt; k += G) {
           const float4 bh = ss[wi][k].hi;
