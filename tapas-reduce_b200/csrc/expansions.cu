@@ -385,11 +385,15 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
 // L2P of the mixed form in FP32: the local expansion's terms fall off
 // geometrically inside the leaf, so one FP32 evaluation of them is accurate
 // to ~1e-7 of the far-field potential; the result is added into the FP64
-// totals.
+// totals.  The evaluation runs in units of the leaf width w (L'_n = L_n w^n,
+// r' = r / w: every term L Y_n^m(r) is unchanged, the gradient is scaled by
+// 1/w at the end), which keeps every FP32 quantity bounded; L_n itself grows
+// like 1/R^(n+1) and leaves the FP32 range at high n in small cells.
 template <int P>
 __global__ void __launch_bounds__(kThreads) l2p32_kernel(
     const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
     const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
+    const double *__restrict__ cmin, const double *__restrict__ cmax,
     const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
     const double *__restrict__ sq, const double2 *__restrict__ L, double *__restrict__ trg,
     int near_has_q) {
@@ -401,15 +405,21 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
   const int c = leaves[w];
   const int b0 = cbeg[c], nb = cnb[c];
   float2 *Lc = Lsm[wi];
+  const double width = cmax[3 * c] - cmin[3 * c], iw = 1.0 / width;
   for (int t = lane; t < S::NT; t += 32) {
+    int n, m;
+    jk_of(t, n, m);
+    double wn = 1.0;
+    for (int k = 0; k < n; k++) wn *= width;
     const double2 v = L[(int64_t)c * S::NT + t];
-    Lc[t] = make_float2((float)v.x, (float)v.y);
+    Lc[t] = make_float2((float)(v.x * wn), (float)(v.y * wn));
   }
   __syncwarp();
   const double cx = ccen[3 * c], cy = ccen[3 * c + 1], cz = ccen[3 * c + 2];
   for (int b = lane; b < nb; b += 32) {
     const int64_t bi = b0 + b;
-    const float dx = (float)(sx[bi] - cx), dy = (float)(sy[bi] - cy), dz = (float)(sz[bi] - cz);
+    const float dx = (float)((sx[bi] - cx) * iw), dy = (float)((sy[bi] - cy) * iw),
+                dz = (float)((sz[bi] - cz) * iw);
     // cart2sph (:43-47): r, cos/sin of theta and e^{i phi} from the offset
     const float rxy2 = dx * dx + dy * dy;
     const float r = sqrtf(rxy2 + dz * dz);
@@ -481,9 +491,9 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
     // its `ba /= b.SRC`)
     const double iq = near_has_q ? 1.0 / sq[bi] : 1.0;
     o[0] = o[0] * iq + (double)pot;
-    o[1] = o[1] * iq + (double)c0;
-    o[2] = o[2] * iq + (double)c1;
-    o[3] = o[3] * iq + (double)c2;
+    o[1] = o[1] * iq + (double)c0 * iw;
+    o[2] = o[2] * iq + (double)c1 * iw;
+    o[3] = o[3] * iq + (double)c2 * iw;
   }
 }
 
@@ -875,7 +885,8 @@ int downward_P(tapas_b200_ctx *ctx, bool l2p_f32) {
   const int64_t nl = ctx->n_nonempty_leaves;
   if (nl > 0 && l2p_f32) {
     l2p32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
+        ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
+        ctx->sx.p, ctx->sy.p,
         ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p,
         ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
     TB_LAUNCH_CHECK(ctx);

@@ -98,6 +98,9 @@ def generate(n_systems=250, per_system=8, seed_base=10_000, out=DATA_PATH, n_lar
                         if attempt == 3:
                             raise
                 err = verify.rel_l2(res[tg], d)[0]
+                if not (np.isfinite(err) and np.isfinite(ms)):
+                    raise RuntimeError(f"system {k} n={n} {dist} P={P} theta={theta} "
+                                       f"ncrit={ncrit} fp64={fp64}: non-finite result")
                 rows.append(np.concatenate([feats, [P, theta, ncrit, fp64,
                                                     np.log10(max(err, 1e-16)),
                                                     np.log10(ms), n, DISTS.index(dist)]]))

@@ -185,6 +185,20 @@ def test_mixed_close_to_fp64(dist, ncrit, tb, ctx, oracle_mod):
     assert emx[0] < 1.5 * e64[0] + 1e-6 and emx[1] < 1.5 * e64[1] + 1e-6
 
 
+@pytest.mark.parametrize("P", [14, 16])
+def test_mixed_high_order_deep_tree(P, tb, ctx, oracle_mod):
+    """Mixed form at high order on a deep tree: in small cells the local
+    coefficients of degree n grow like 1/R^(n+1), beyond the FP32 range, so
+    the FP32 L2P must work in units of the leaf width.  The results are finite
+    and within 2e-6 (rel-L2) of the FP64 form."""
+    x, y, z, q = tb.datasets.make("two_gaussians", 200000, 7)
+    r64 = ctx.evaluate(x, y, z, q, P=P, ncrit=32, theta=0.4, precision=tb.FP64)
+    rmx = ctx.evaluate(x, y, z, q, P=P, ncrit=32, theta=0.4, precision=tb.MIXED)
+    assert np.isfinite(rmx).all()
+    ep, ea = oracle_mod.rel_l2(rmx, r64)
+    assert ep < 2e-6 and ea < 2e-6
+
+
 @pytest.mark.parametrize("P", [4, 6, 8, 10, 11, 12, 14, 16])
 def test_tensorcore_m2l_matches_fp64(P, tb, ctx):
     """Split-TF32 tensor-core M2L (mixed) against the FP64 M2L: per cell,
