@@ -17,13 +17,14 @@ from __future__ import annotations
 
 
 # DRAM bytes of one p2p_mixed_kernel launch per body, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum = 47.4 MB + 11.5 MB on a 1M-body
-# unit-sphere-surface set, P=10, theta=0.25, ncrit=128).  The kernel's DRAM
+# (dram__bytes_read.sum + dram__bytes_write.sum = 40.6 MB + 8.8 MB on a 1M-body
+# unit-sphere-surface set, P=15, theta=0.4, ncrit=128).  The kernel's DRAM
 # traffic is its body arrays read and results written (its source re-reads hit
 # L2), so a launch's traffic is this figure times the bodies.
-P2P_MIXED_DRAM_BYTES_PER_BODY = 58.9
-# Same capture, m2l_tc_kernel<10>: 531 MB + 8.7 MB for 2.67M translations.
-M2L_TC_DRAM_BYTES_PER_TRANSLATION = 202.0
+P2P_MIXED_DRAM_BYTES_PER_BODY = 49.4
+# Same capture, m2l_tc_kernel<15>: 540.5 MB + 45.8 MB for 1.04M translations
+# (the operator and multipole rows grow with P).
+M2L_TC_DRAM_BYTES_PER_TRANSLATION = 565.0
 
 
 def m2l_flops_per_translation(P: int) -> int:
