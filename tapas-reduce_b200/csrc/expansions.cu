@@ -1,4 +1,4 @@
-// FP64 expansion kernels: P2M, M2M, M2L, L2L, L2P (ExaFMM Laplace spherical
+// Expansion kernels: P2M, M2M, M2L, L2L, L2P (ExaFMM Laplace spherical
 // harmonics, ex/LaplaceSphericalCPU_tapas.h), templated on the order P.
 //
 // Work mapping:
@@ -12,6 +12,9 @@
 //   L2L  - per level, one FP64 GEMM as M2M, parents to stacked children.
 //   L2P  - warp per non-empty leaf; lane per body, harmonics streamed in
 //          registers (no table), L of the leaf staged in shared memory.
+// Mixed form only: m2l_pair_kernel (the FP64 M2L of the pairs the tensor cores
+// leave, one warp per pair) and l2p32_kernel (L2P in FP32, in units of the
+// leaf width).
 #include "expansions.cuh"
 #include "kernels.cuh"
 
