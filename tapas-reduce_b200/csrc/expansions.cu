@@ -146,6 +146,125 @@ __global__ void __launch_bounds__(kThreads) p2m_kernel(
   }
 }
 
+// warp_reduce_scatter16 for FP32 values (half the shuffles of the FP64 one).
+__device__ __forceinline__ float warp_reduce_scatter16f(float (&buf)[16], int lane) {
+#pragma unroll
+  for (int o = 16, h = 8; o >= 2; o >>= 1, h >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; i++) {
+      const float keep = up ? buf[i + h] : buf[i];
+      const float send = up ? buf[i] : buf[i + h];
+      buf[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return buf[0] + __shfl_xor_sync(0xffffffffu, buf[0], 1);
+}
+
+// P2M of the mixed form: each body's terms in FP32, in units of the leaf width
+// w (rho' = rho / w <= ~0.87, so rho'^n stays in range at every n; M_n = w^n
+// times the sum), 8 complex terms at a time summed over the warp by one
+// FP32 reduce-scatter, the sums over body chunks and the output in FP64.  A
+// term's rounding is ~6e-8 of itself and the warp's tree sum adds ~5 such
+// roundings, so M keeps ~1e-7 relative accuracy also when zero-mean charges
+// cancel.
+template <int P>
+__global__ void __launch_bounds__(kThreads) p2m32_kernel(
+    const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
+    const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
+    const double *__restrict__ cmin, const double *__restrict__ cmax,
+    const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
+    const double *__restrict__ sq, double2 *__restrict__ M) {
+  using S = Sizes<P>;
+  constexpr int kGroups = (S::NT + 7) / 8;  // 8 complex terms per reduction
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int b0 = cbeg[c], nb = cnb[c];
+  const double cx = ccen[3 * c], cy = ccen[3 * c + 1], cz = ccen[3 * c + 2];
+  const double width = cmax[3 * c] - cmin[3 * c], iw = 1.0 / width;
+  double acc[kGroups];  // lane l: component of slot (l >> 1) & 15 of group g
+#pragma unroll
+  for (int g = 0; g < kGroups; g++) acc[g] = 0;
+  for (int base = 0; base < nb; base += 32) {
+    const int b = base + lane;
+    float q = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
+    if (b < nb) {
+      q = (float)sq[b0 + b];
+      dx = (float)((sx[b0 + b] - cx) * iw);
+      dy = (float)((sy[b0 + b] - cy) * iw);
+      dz = (float)((sz[b0 + b] - cz) * iw);
+    }
+    // cart2sph (:43-47): rho', cos/sin of alpha and e^{i beta} from the offset
+    const float rxy2 = dx * dx + dy * dy;
+    const float rho = sqrtf(rxy2 + dz * dz);
+    float x = 1.f, y = 0.f, eix = 1.f, eiy = 0.f;
+    if (rho > 0.f) {
+      const float rxy = sqrtf(rxy2);
+      x = dz / rho;
+      y = rxy / rho;
+      if (rxy > 0.f) {
+        eix = dx / rxy;
+        eiy = dy / rxy;
+      }
+    }
+    float buf[16];
+    int s = 0;
+    float fact = 1.f, pn = 1.f, rhom = 1.f;
+    float emx = 1.f, emy = 0.f;  // e^{i m beta}
+#pragma unroll
+    for (int m = 0; m < P; m++) {
+      float p = pn, p1 = pn;
+      float rhon = rhom;
+#pragma unroll
+      for (int n = m; n < P; n++) {
+        if (n > m) rhon *= 1.f / (float)(-(n + m));  // constants after unrolling
+        const float sc = q * rhon * p;
+        buf[2 * (s & 7)] = sc * emx;
+        buf[2 * (s & 7) + 1] = -sc * emy;
+        if ((s & 7) == 7 || s == S::NT - 1) {
+#pragma unroll
+          for (int i = 2 * (s & 7) + 2; i < 16; i++) buf[i] = 0.f;
+          acc[s >> 3] += (double)warp_reduce_scatter16f(buf, lane);
+        }
+        s++;
+        if (n == m) {
+          p = x * (float)(2 * m + 1) * p1;
+          rhon = rhom * rho;
+        } else {
+          const float p2 = p1;
+          p1 = p;
+          p = (x * (float)(2 * n + 1) * p1 - (float)(n + m) * p2) * (1.f / (float)(n - m + 1));
+          rhon *= rho;
+        }
+      }
+      rhom = rhom * rho * (1.f / (float)(-(2 * m + 2) * (2 * m + 1)));
+      pn = -pn * fact * y;
+      fact += 2.f;
+      const float ex = emx * eix - emy * eiy;
+      emy = emx * eiy + emy * eix;
+      emx = ex;
+    }
+  }
+  double *Mc = reinterpret_cast<double *>(M + (int64_t)c * S::NT);
+  const int d = (lane >> 1) & 15;
+  if ((lane & 1) == 0) {
+#pragma unroll
+    for (int g = 0; g < kGroups; g++) {
+      const int sp = 8 * g + (d >> 1);
+      if (sp < S::NT) {
+        const int t = p2m_term_index<P>(sp);
+        int n, m;
+        jk_of(t, n, m);
+        double wn = 1.0;
+        for (int k = 0; k < n; k++) wn *= width;
+        Mc[2 * t + (d & 1)] = acc[g] * wn;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // M2L (:208-273, mutual = 0): L[t] = sum over sources s of T(c_t - c_s) M[s]
 // ---------------------------------------------------------------------------
@@ -806,7 +925,7 @@ int level_translate(tapas_b200_ctx *ctx, int l, const LevelFirstChild &lf, bool 
 }
 
 template <int P>
-int upward_P(tapas_b200_ctx *ctx) {
+int upward_P(tapas_b200_ctx *ctx, bool p2m_f32) {
   using S = Sizes<P>;
   cudaStream_t s = ctx->stream;
   const int64_t C = ctx->ncells;
@@ -815,7 +934,12 @@ int upward_P(tapas_b200_ctx *ctx) {
   {
     PhaseTimer t(ctx, &ctx->timings.p2m);
     const int64_t nl = ctx->n_nonempty_leaves;
-    if (nl > 0) {
+    if (nl > 0 && p2m_f32) {
+      p2m32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+          ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
+          ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->M.p);
+      TB_LAUNCH_CHECK(ctx);
+    } else if (nl > 0) {
       p2m_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
           ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
           ctx->sz.p, ctx->sq.p, ctx->M.p);
@@ -916,7 +1040,12 @@ int downward_P(tapas_b200_ctx *ctx, bool l2p_f32) {
   set_error(ctx, "expansion order P=%d outside %d..%d", (P), kMinP, kMaxP);          \
   return TAPAS_B200_ERR_UNSUPPORTED;
 
-int upward_fp64(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_P) }
+template <int P>
+int upward_fp64_P(tapas_b200_ctx *ctx) { return upward_P<P>(ctx, false); }
+template <int P>
+int upward_f32leaf_P(tapas_b200_ctx *ctx) { return upward_P<P>(ctx, true); }
+int upward_fp64(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_fp64_P) }
+int upward_fp32_p2m(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_f32leaf_P) }
 int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
 
 static int m2l_pairs_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_pairs_P) }

@@ -5,6 +5,8 @@
 namespace tb {
 // FP64 expansion passes (expansions.cu); P in [kMinP, kMaxP].
 int upward_fp64(tapas_b200_ctx *ctx, int P);
+// P2M in FP32 (FP64 sums and output), then FP64 M2M.
+int upward_fp32_p2m(tapas_b200_ctx *ctx, int P);
 int m2l_fp64(tapas_b200_ctx *ctx);
 // L zeroed, then the FP64 M2L of the pairs at list indices pairs[0..npairs)
 // added into it (atomics: the order of a target's sums is not fixed).

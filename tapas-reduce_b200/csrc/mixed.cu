@@ -10,7 +10,7 @@
 
 namespace tb {
 
-int upward_mixed(tapas_b200_ctx *ctx, int P) { return upward_fp64(ctx, P); }
+int upward_mixed(tapas_b200_ctx *ctx, int P) { return upward_fp32_p2m(ctx, P); }
 
 int m2l_mixed(tapas_b200_ctx *ctx) { return m2l_tensorcore(ctx); }
 
