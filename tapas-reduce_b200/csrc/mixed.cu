@@ -1,9 +1,10 @@
 // Mixed-precision evaluation path (TAPAS_B200_MIXED).
 //
 // Near field: FP32 compensated P2P (p2p.cu, p2p_mixed).  M2L: offset-class
-// batched split-TF32 GEMMs on the tensor cores (m2l_tc.cu).  Upward pass and
-// L2L stay FP64; L2P runs in FP32 and adds to the near-field result, which is
-// per unit charge (so without the reference's division by q_i).
+// batched split-TF32 GEMMs on the tensor cores (m2l_tc.cu).  P2M and L2P run
+// in FP32 in units of the leaf width (FP64 sums and outputs); M2M and L2L stay
+// FP64.  L2P adds to the near-field result, which is per unit charge (so
+// without the reference's division by q_i).
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
 #include "mixed.cuh"
