@@ -48,8 +48,9 @@ enum { TAPAS_B200_HOST = 0, TAPAS_B200_DEVICE = 1 };
 /* Arithmetic of the expansion and near-field kernels. */
 enum {
   TAPAS_B200_FP64 = 0,  /* plain FP64 everywhere (the reference's FP64 build)          */
-  TAPAS_B200_MIXED = 1  /* FP32 compensated P2P, split-precision tensor-core M2L,
-                           FP64 M2M/L2L at tree levels <= 3 and FP64 final sums        */
+  TAPAS_B200_MIXED = 1  /* FP32 compensated P2P; FP32 P2M and L2P in units of the leaf
+                           width; split-TF32 tensor-core M2L (FP64 for rare offset
+                           classes); FP64 M2M/L2L; FP64 sums and outputs               */
 };
 
 /* Output order of per-body results. */
@@ -106,6 +107,14 @@ int tapas_b200_set_profiling(tapas_b200_ctx *ctx, int on);
  * nothing, are dropped.  Results are the same either way. */
 int tapas_b200_set_reference_lists(tapas_b200_ctx *ctx, int on);
 int tapas_b200_get_timings(tapas_b200_ctx *ctx, tapas_b200_timings *out);
+/* Bound, in GPU clock cycles, on each wait between the roles of the
+ * tensor-core M2L kernel (copy ring, MMA issue, epilogue); cycles <= 0 restores
+ * the default 4e9 (about 2 s).  A wait that runs out makes the kernel drain its
+ * copies and MMAs, free its tensor memory and return, and the call returns
+ * TAPAS_B200_ERR_TIMEOUT with the context still usable.  No counterpart in
+ * the reference (its GPU path has no bounded waits); meant for tests of that
+ * failure path and for callers that want a shorter watchdog. */
+int tapas_b200_set_wait_limit(tapas_b200_ctx *ctx, int64_t cycles);
 /* Message of the last failing call on this context ("" if none). Thread-local
  * fallback when ctx is NULL (e.g. ctx_create failure). */
 const char *tapas_b200_last_error(const tapas_b200_ctx *ctx);
@@ -194,8 +203,12 @@ int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision);
  * body-pair offload (hot/mapper.h:453-690, vectormap_cuda.h:826-1005):
  * builds the M2L and P2P lists with the FMM_DTT acceptance test and split
  * rule (:209-286) and evaluates M2L (LaplaceSphericalCPU_tapas.h:208-273) and
- * P2P (LaplaceP2PCPU_tapas.h:23-74).  mutual must be 0, as in the reference's
- * CUDA build (ex/tapas_exafmm.cxx:507-515). */
+ * P2P (LaplaceP2PCPU_tapas.h:23-74).
+ * mutual = 1 is the example's -m option, which the reference's CPU build runs
+ * (its CUDA build rejects it, ex/tapas_exafmm.cxx:507-515): every unordered
+ * cell pair is visited once (a cell with itself splits both sides and visits
+ * child pairs i <= j) and acts both ways.  The lists then hold both directions
+ * of each visited pair, and the results are the reference's -m 1 results. */
 int tapas_b200_traverse(tapas_b200_ctx *ctx, double theta, int mutual, int precision);
 /* The same, in steps: list construction only, then each list. */
 int tapas_b200_build_lists(tapas_b200_ctx *ctx, double theta, int mutual);
@@ -231,6 +244,46 @@ int tapas_b200_evaluate(tapas_b200_ctx *ctx, const double *x, const double *y, c
  * Bodies are the ones of the last partition; targets are original indices. */
 int tapas_b200_direct(tapas_b200_ctx *ctx, const int64_t *targets, int64_t k, double *out4,
                       int mem);
+
+/* ---- file formats (host code; no GPU needed) ------------------------------ */
+
+/* Body files of the reference's Dataset (exafmm include/dataset.h:313-372):
+ * <dir>/source%04d.dat (rank) holds x, y, z, q of each body, one value per
+ * line; <dir>/target%04d.dat holds pot, ax, ay, az.  dir NULL or "" = the
+ * working directory.  Writers: digits <= 0 formats as the reference does (the
+ * stream default, 6 significant digits), digits > 0 sets the precision (17
+ * round-trips FP64).  Readers read n bodies starting at *position (a byte
+ * offset; NULL = the file's start) and store the position after them there,
+ * so successive calls continue through the file as the reference's
+ * readSources/readTargets do with Dataset::filePosition.  trg4 is 4 values per
+ * body.  Errors: tapas_b200_last_error(NULL). */
+int tapas_b200_write_sources(const char *dir, int rank, int64_t n, const double *x,
+                             const double *y, const double *z, const double *q, int digits);
+int tapas_b200_write_targets(const char *dir, int rank, int64_t n, const double *trg4,
+                             int digits);
+int tapas_b200_read_sources(const char *dir, int rank, int64_t n, double *x, double *y,
+                            double *z, double *q, int64_t *position);
+int tapas_b200_read_targets(const char *dir, int rank, int64_t n, double *trg4,
+                            int64_t *position);
+
+/* The example's per-step report (ex/tapas_exafmm.cxx:651-677; RankCSV of
+ * cpp/include/tapas/util.h:223-316): writes `path` with the columns Rank,
+ * total, upward, traverse, downward, tree (seconds), numP2P, numM2L (the
+ * -DCOUNT counters) in the reference's fixed-width layout. */
+int tapas_b200_write_main_csv(const char *path, int rank, double total, double upward,
+                              double traverse, double downward, double tree, uint64_t num_p2p,
+                              uint64_t num_m2l);
+/* Replaces the example's report of a timestep (main.csv, :651-677) and
+ * Cell::Report (hot/report.h:40-152: hostnames, misc, load_balancing,
+ * tree_construction, map2 .csv; the sampling, exchange and LET columns are 0
+ * on one GPU) for the context's last evaluation, into files
+ * <prefix><name><suffix>.csv (NULL prefix/suffix: the environment variables
+ * TAPAS_REPORT_PREFIX / TAPAS_REPORT_SUFFIX, as the reference reads them).
+ * Times come from the phase timings, so turn profiling on
+ * (tapas_b200_set_profiling) before the evaluation; otherwise they are 0.
+ * numP2P / numM2L count functor calls as the reference does: they equal the
+ * reference's counters for lists built with tapas_b200_set_reference_lists(1). */
+int tapas_b200_write_report(tapas_b200_ctx *ctx, const char *prefix, const char *suffix);
 
 /* The same FP64 direct-sum check, for callers that must not allocate device
  * memory at the point where they verify accuracy: a solver loop that reserved

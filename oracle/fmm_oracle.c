@@ -126,6 +126,7 @@ struct oracle_fmm {
   int64_t n;
   int P, nterm, ncrit;
   double theta;
+  int mutual;                     /* the example's -m option (0 or 1) */
   double *x, *y, *z, *q;          /* original order */
   double *sx, *sy, *sz, *sq;      /* sorted order */
   int64_t *perm;                  /* sorted position -> original index */
@@ -487,48 +488,63 @@ int oracle_upward(oracle_fmm *h) {
   return 0;
 }
 
-/* M2L with mutual = 0, :208-273 */
+/* M2L, :208-273.  With mutual the same call also translates Ci's multipole
+ * into Cj's local expansion, from the harmonics at (rho, alpha + pi, beta)
+ * (:222-223), accumulated in the same loop (:244-263). */
 static void m2l(oracle_fmm *h, int32_t ti, int32_t si) {
   const ocell *Ci = &h->cells[ti], *Cj = &h->cells[si];
   int P = h->P;
+  const int mutual = h->mutual;
   cplx *Li = h->L + (size_t)ti * h->nterm;
+  cplx *Lj = h->L + (size_t)si * h->nterm;
+  const cplx *Mi = h->M + (size_t)ti * h->nterm;
   const cplx *Mj = h->M + (size_t)si * h->nterm;
   double dX[3] = {Ci->center[0] - Cj->center[0], Ci->center[1] - Cj->center[1],
                   Ci->center[2] - Cj->center[2]};
   double rho, alpha, beta;
   cart2sph(&rho, &alpha, &beta, dX);
   eval_local(P, rho, alpha, beta, h->ynm);
+  if (mutual) eval_local(P, rho, alpha + M_PI, beta, h->ynmt);
   for (int j = 0; j < P; j++) {
     double Cnm = ODDEVEN(j);
     for (int k = 0; k <= j; k++) {
       int jks = j * (j + 1) / 2 + k;
-      cplx acc = 0;
+      cplx acc = 0, accj = 0;
       for (int n = 0; n < P - j; n++) {
         for (int m = -n; m < 0; m++) {
           int nms = n * (n + 1) / 2 - m;
           int jnkm = (j + n) * (j + n) + j + n + m - k;
           acc += conj(Mj[nms]) * Cnm * h->ynm[jnkm];
+          if (mutual) accj += conj(Mi[nms]) * Cnm * h->ynmt[jnkm];
         }
         for (int m = 0; m <= n; m++) {
           int nms = n * (n + 1) / 2 + m;
           int jnkm = (j + n) * (j + n) + j + n + m - k;
           double Cnm2 = Cnm * ODDEVEN((k - m) * (k < m) + m);
           acc += Mj[nms] * Cnm2 * h->ynm[jnkm];
+          if (mutual) accj += Mi[nms] * Cnm2 * h->ynmt[jnkm];
         }
       }
       Li[jks] += acc;
+      if (mutual) Lj[jks] += accj;
     }
   }
 }
 
-/* P2P functor (CPU form, mutual = 0), ex/LaplaceP2PCPU_tapas.h:48-74, over
- * the body double loop of hot/mapper.h:127-169 (targets outer). EPS2 = 0. */
+/* P2P functor (CPU form), ex/LaplaceP2PCPU_tapas.h:48-74, over the body double
+ * loop of hot/mapper.h:127-169 (targets outer). EPS2 = 0.  With mutual, a leaf
+ * with itself visits j <= i only (AllowMutualInteraction, iterator.h:98-100)
+ * and every pair also updates body j (`mutual && Bi.X != Bj.X`: the vec's
+ * pointer conversion makes that "j is another body object"). */
 static void p2p(oracle_fmm *h, int32_t ti, int32_t si) {
   const ocell *Ci = &h->cells[ti], *Cj = &h->cells[si];
+  const int mutual = h->mutual;
+  const int tri = mutual && ti == si;
   for (int64_t a = 0; a < Ci->nb; a++) {
     int64_t i = Ci->bbeg + a;
     double *t = h->trg + 4 * i;
-    for (int64_t b = 0; b < Cj->nb; b++) {
+    const int64_t bend = tri ? a + 1 : Cj->nb;
+    for (int64_t b = 0; b < bend; b++) {
       int64_t j = Cj->bbeg + b;
       double dX[3] = {h->sx[i] - h->sx[j] - 0.0, h->sy[i] - h->sy[j] - 0.0,
                       h->sz[i] - h->sz[j] - 0.0};
@@ -546,6 +562,13 @@ static void p2p(oracle_fmm *h, int32_t ti, int32_t si) {
         t[1] -= dX[0];
         t[2] -= dX[1];
         t[3] -= dX[2];
+        if (mutual && i != j) {
+          double *u = h->trg + 4 * j;
+          u[0] += invR;
+          u[1] += dX[0];
+          u[2] += dX[1];
+          u[3] += dX[2];
+        }
       }
     }
   }
@@ -560,8 +583,36 @@ static void push_pair(int32_t **t, int32_t **s, int64_t *n, int64_t *cap, int32_
   (*t)[*n] = a; (*s)[*n] = b; (*n)++;
 }
 
-/* FMM_DTT, ex/tapas_exafmm.cxx:209-286, mutual = 0.  R2 is the squared
- * centre distance (geometry.h:81-83 via tapas Vec::norm, vec.h:52-58). */
+static void dtt(oracle_fmm *h, int32_t ti, int32_t si);
+
+/* ProductMapImpl (hot/mapper.h:28-121) over a cell's subcells with
+ * themselves under mutual: pairs (i, j) with i <= j.  SubCellIterator spawns
+ * (splits the ranges) when the parent holds >= 1000 bodies (iterator.h:203-205)
+ * and runs ranges of <= 2 (kThreadSpawnThreshold, :199-201) serially; a split
+ * visits (lo, lo), (hi, hi), then (lo, hi), (hi, lo), and the Serial task
+ * group runs each task as it is created (threading/serial.h). */
+static void self_product(oracle_fmm *h, const int32_t *ch, int spawn, int b1, int e1, int b2,
+                         int e2) {
+  if (!spawn || e1 - b1 == 1 || (e1 - b1 <= 2 && e2 - b2 <= 2)) {
+    for (int i = b1; i < e1; i++)
+      for (int j = b2; j < e2; j++)
+        if (i <= j) dtt(h, ch[i], ch[j]);
+  } else if (e2 - b2 == 1) {
+    const int m1 = (b1 + e1) / 2;
+    self_product(h, ch, spawn, b1, m1, b2, e2);
+    self_product(h, ch, spawn, m1, e1, b2, e2);
+  } else {
+    const int m1 = (b1 + e1) / 2, m2 = (b2 + e2) / 2;
+    self_product(h, ch, spawn, b1, m1, b2, m2);
+    self_product(h, ch, spawn, m1, e1, m2, e2);
+    self_product(h, ch, spawn, b1, m1, m2, e2);
+    self_product(h, ch, spawn, m1, e1, b2, m2);
+  }
+}
+
+/* FMM_DTT, ex/tapas_exafmm.cxx:209-286.  R2 is the squared centre distance
+ * (geometry.h:81-83 via tapas Vec::norm, vec.h:52-58).  The lists record the
+ * visited pairs (with mutual: each unordered pair once, as visited). */
 static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
   const ocell *Ci = &h->cells[ti], *Cj = &h->cells[si];
   double dc[3] = {Ci->center[0] - Cj->center[0], Ci->center[1] - Cj->center[1],
@@ -585,11 +636,14 @@ static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
     /* tapas::Map over an empty body product is skipped (hot.h:1362-1369). */
     if (Ci->nb > 0 && Cj->nb > 0) {
       push_pair(&h->p2p_t, &h->p2p_s, &h->np2p, &h->cp2p, ti, si);
-      h->np2p_int += (uint64_t)(Ci->nb * Cj->nb);
+      /* the functor calls the reference counts (INC_P2P): j <= i within a
+       * leaf under mutual */
+      h->np2p_int += (h->mutual && ti == si) ? (uint64_t)(Ci->nb * (Ci->nb + 1) / 2)
+                                              : (uint64_t)(Ci->nb * Cj->nb);
       p2p(h, ti, si);
     }
   } else {
-    /* tapas_splitCell, :252-285 (mutual = 0; ties split Ci). */
+    /* tapas_splitCell, :252-285 (ties split Ci). */
     int ci_leaf = Ci->leaf, cj_leaf = Cj->leaf;
     int32_t chi[8], chj[8];
     memcpy(chi, Ci->child, sizeof chi);
@@ -598,6 +652,10 @@ static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
       for (int c = 0; c < 8; c++) dtt(h, chi[c], si);
     } else if (ci_leaf) {
       for (int c = 0; c < 8; c++) dtt(h, ti, chj[c]);
+    } else if (h->mutual && ti == si) {
+      /* both sides split; the product of a cell's subcells with themselves
+       * visits (i, j) for i <= j only, in ProductMapImpl's order */
+      self_product(h, chi, Ci->nb >= 1000, 0, 8, 0, 8);
     } else if (Ri >= Rj) {
       for (int c = 0; c < 8; c++) dtt(h, chi[c], si);
     } else {
@@ -605,6 +663,8 @@ static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
     }
   }
 }
+
+void oracle_set_mutual(oracle_fmm *h, int mutual) { h->mutual = mutual != 0; }
 
 int oracle_traverse(oracle_fmm *h) {
   if (!h->cells) return -1;

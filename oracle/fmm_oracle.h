@@ -34,6 +34,9 @@ void oracle_destroy(oracle_fmm *h);
 int oracle_build(oracle_fmm *h);     /* bbox, keys, sort, cell tree       */
 int oracle_upward(oracle_fmm *h);    /* P2M + M2M                          */
 int oracle_traverse(oracle_fmm *h);  /* dual-tree traversal: M2L + P2P     */
+/* The example's -m option: mutual = 1 visits each unordered cell pair once
+ * and applies M2L and P2P both ways (set before oracle_traverse). */
+void oracle_set_mutual(oracle_fmm *h, int mutual);
 int oracle_downward(oracle_fmm *h);  /* L2L + L2P                          */
 int oracle_run_all(oracle_fmm *h);
 

@@ -37,7 +37,8 @@ def build(quiet: bool = True) -> None:
 
 
 def build_reference(quiet: bool = True) -> bool:
-    ref = os.environ.get("TAPAS_REFERENCE_ROOT", "/root/reference")
+    # the reference checkout: TAPAS_REFERENCE_ROOT, else a sibling of this repository
+    ref = os.environ.get("TAPAS_REFERENCE_ROOT", str(HERE.parent.parent / "reference"))
     if not pathlib.Path(ref, "cpp", "include", "tapas.h").exists():
         return False
     out = subprocess.DEVNULL if quiet else None
@@ -59,6 +60,8 @@ def lib():
             getattr(L, f).argtypes = [_vp]
             getattr(L, f).restype = ctypes.c_int
         L.oracle_destroy.argtypes = [_vp]
+        L.oracle_set_mutual.argtypes = [_vp, ctypes.c_int]
+        L.oracle_set_mutual.restype = None
         for f in ("oracle_ncells", "oracle_n_m2l", "oracle_n_p2p"):
             getattr(L, f).argtypes = [_vp]
             getattr(L, f).restype = _c_i64
@@ -100,14 +103,15 @@ def _p(a: np.ndarray):
 class Oracle:
     """One FMM evaluation by the CPU restatement (fmm_oracle.c)."""
 
-    def __init__(self, x, y, z, q, P=10, ncrit=64, theta=0.4, run=True):
+    def __init__(self, x, y, z, q, P=10, ncrit=64, theta=0.4, run=True, mutual=0):
         L = lib()
         self._keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
         self.n = len(self._keep[0])
-        self.P, self.ncrit, self.theta = P, ncrit, theta
+        self.P, self.ncrit, self.theta, self.mutual = P, ncrit, theta, int(mutual)
         self.h = L.oracle_create(self.n, *[_p(a) for a in self._keep], P, ncrit, float(theta))
         if not self.h:
             raise ValueError("oracle_create rejected its arguments")
+        L.oracle_set_mutual(self.h, int(mutual))
         if run:
             rc = L.oracle_run_all(self.h)
             if rc != 0:
@@ -283,7 +287,7 @@ def read_reference_output(path):
                 bodies=bodies, cells=cells)
 
 
-def run_reference(x, y, z, q, P=10, ncrit=64, theta=0.4, repeat=1, timeout=3600):
+def run_reference(x, y, z, q, P=10, ncrit=64, theta=0.4, repeat=1, timeout=3600, mutual=0):
     exe = reference_binary(P)
     if not exe.exists():
         raise FileNotFoundError(f"{exe} not built (make -C oracle ref)")
@@ -291,6 +295,6 @@ def run_reference(x, y, z, q, P=10, ncrit=64, theta=0.4, repeat=1, timeout=3600)
         fi = os.path.join(d, "in.bin")
         fo = os.path.join(d, "out.bin")
         write_input(fi, x, y, z, q, ncrit, theta)
-        subprocess.run([str(exe), fi, fo, str(repeat)], check=True, timeout=timeout,
-                       stdout=subprocess.DEVNULL)
+        subprocess.run([str(exe), fi, fo, str(repeat), str(int(mutual))], check=True,
+                       timeout=timeout, stdout=subprocess.DEVNULL)
         return read_reference_output(fo)

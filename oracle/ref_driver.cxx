@@ -11,8 +11,10 @@
 // It is test infrastructure: built by oracle/Makefile into oracle/_ref/, run
 // only by tests/, tests/golden/make_golden.py and bench.py's reference arm.
 //
-// Usage:  tapas_exafmm_ref IN OUT [repeat]
+// Usage:  tapas_exafmm_ref IN OUT [repeat [mutual]]
 //   IN : int64 n, int32 ncrit, float64 theta, then n x {x,y,z,q} float64
+//   mutual: 0 (default) or 1, the example's -m option (SetOptMutual and the
+//           FMM_DTT mutual argument, tapas_exafmm.cxx:507-515,604-606)
 //   OUT: see write_output() below.
 
 #define main tapas_exafmm_reference_main
@@ -62,10 +64,11 @@ void put(FILE *f, const T &v) { fwrite(&v, sizeof(T), 1, f); }
 
 int main(int argc, char **argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s IN OUT [repeat]\n", argv[0]);
+    fprintf(stderr, "usage: %s IN OUT [repeat [mutual]]\n", argv[0]);
     return 2;
   }
   int repeat = argc > 3 ? atoi(argv[3]) : 1;
+  const int mutual = argc > 4 ? (atoi(argv[4]) != 0) : 0;
   Bodies input;
   int ncrit = 0;
   double theta = 0;
@@ -87,13 +90,13 @@ int main(int argc, char **argv) {
     root = TapasFMM::Partition(bodies.data(), bodies.size(), ncrit);
     double et = GetTime();
     double tt = et - bt;
-    root->SetOptMutual(0);
+    root->SetOptMutual(mutual);
     bt = GetTime();
     TapasFMM::Map(FMM_Upward(), *root, (real_t)theta);
     et = GetTime();
     double tu = et - bt;
     bt = GetTime();
-    TapasFMM::Map(FMM_DTT(), tapas::Product(*root, *root), 0, 0, (real_t)theta);
+    TapasFMM::Map(FMM_DTT(), tapas::Product(*root, *root), mutual, 0, (real_t)theta);
     et = GetTime();
     double td = et - bt;
     bt = GetTime();

@@ -14,8 +14,10 @@ Importing the package never falls back to a CPU path: without the built
 library, ``Context`` raises.
 """
 from ._lib import (DEVICE, FP64, HOST, MIXED, ORDER_ORIGINAL, ORDER_SORTED, Context,  # noqa: F401
-                   TapasError, lib)
+                   TapasError, lib, read_sources, read_targets, write_main_csv, write_sources,
+                   write_targets)
 from . import datasets  # noqa: F401
 
 __all__ = ["Context", "TapasError", "lib", "datasets", "FP64", "MIXED", "HOST", "DEVICE",
-           "ORDER_SORTED", "ORDER_ORIGINAL"]
+           "ORDER_SORTED", "ORDER_ORIGINAL", "read_sources", "read_targets", "write_sources",
+           "write_targets", "write_main_csv"]

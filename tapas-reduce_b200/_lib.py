@@ -23,6 +23,7 @@ ORDER_SORTED, ORDER_ORIGINAL = 0, 1
 EXPORTS = (
     "tapas_b200_ctx_create", "tapas_b200_ctx_destroy", "tapas_b200_set_stream",
     "tapas_b200_set_profiling", "tapas_b200_set_reference_lists", "tapas_b200_get_timings",
+    "tapas_b200_set_wait_limit",
     "tapas_b200_last_error",
     "tapas_b200_kernel_launches", "tapas_b200_partition", "tapas_b200_tree_info",
     "tapas_b200_get_cells", "tapas_b200_get_sorted", "tapas_b200_upward",
@@ -34,6 +35,8 @@ EXPORTS = (
     "tapas_b200_mlp_get_params", "tapas_b200_mlp_forward", "tapas_b200_mlp_gradients",
     "tapas_b200_mlp_train", "tapas_b200_bh_upward", "tapas_b200_bh_interact",
     "tapas_b200_bh_counts", "tapas_b200_bh_evaluate",
+    "tapas_b200_write_sources", "tapas_b200_write_targets", "tapas_b200_read_sources",
+    "tapas_b200_read_targets", "tapas_b200_write_main_csv", "tapas_b200_write_report",
 )
 
 
@@ -88,6 +91,7 @@ def lib():
         "tapas_b200_set_stream": [_vp, _vp],
         "tapas_b200_set_profiling": [_vp, _int],
         "tapas_b200_set_reference_lists": [_vp, _int],
+        "tapas_b200_set_wait_limit": [_vp, _i64],
         "tapas_b200_get_timings": [_vp, ctypes.POINTER(Timings)],
         "tapas_b200_partition": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int],
         "tapas_b200_tree_info": [_vp, ctypes.POINTER(TreeStats)],
@@ -127,6 +131,16 @@ def lib():
         "tapas_b200_bh_evaluate": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _dbl, _dbl, _int, _vp,
                                    _int, _int],
     }
+    _cp = ctypes.c_char_p
+    sig2.update({
+        "tapas_b200_write_sources": [_cp, _int, _i64, _vp, _vp, _vp, _vp, _int],
+        "tapas_b200_write_targets": [_cp, _int, _i64, _vp, _int],
+        "tapas_b200_read_sources": [_cp, _int, _i64, _vp, _vp, _vp, _vp, _vp],
+        "tapas_b200_read_targets": [_cp, _int, _i64, _vp, _vp],
+        "tapas_b200_write_main_csv": [_cp, _int, _dbl, _dbl, _dbl, _dbl, _dbl,
+                                      ctypes.c_uint64, ctypes.c_uint64],
+        "tapas_b200_write_report": [_vp, _cp, _cp],
+    })
     for name, args in sig2.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -149,6 +163,58 @@ def _ptr(a):
     if hasattr(a, "data_ptr"):
         return _vp(a.data_ptr()), (DEVICE if a.is_cuda else HOST)
     raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _check_free(rc):
+    """Status of a call that takes no context (message from the thread's last error)."""
+    if rc != OK:
+        msg = lib().tapas_b200_last_error(None)
+        raise TapasError(rc, msg.decode() if msg else "")
+
+
+def _cstr(s):
+    return None if s is None else str(s).encode()
+
+
+# ---- the reference's file formats (host code, no GPU) ------------------------
+def write_sources(directory, rank, x, y, z, q, digits=0):
+    """<directory>/source%04d.dat as the reference's Dataset::writeSources
+    writes it (digits <= 0: its 6-significant-digit default)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
+    _check_free(lib().tapas_b200_write_sources(_cstr(directory), rank, len(arrs[0]),
+                                               *[a.ctypes.data_as(_vp) for a in arrs], digits))
+
+
+def write_targets(directory, rank, trg4, digits=0):
+    t = np.ascontiguousarray(trg4, dtype=np.float64).reshape(-1, 4)
+    _check_free(lib().tapas_b200_write_targets(_cstr(directory), rank, len(t),
+                                               t.ctypes.data_as(_vp), digits))
+
+
+def read_sources(directory, rank, n, position=0):
+    """n bodies from <directory>/source%04d.dat starting at byte `position`:
+    (x, y, z, q, next position)."""
+    arrs = [np.zeros(n) for _ in range(4)]
+    pos = ctypes.c_int64(position)
+    _check_free(lib().tapas_b200_read_sources(_cstr(directory), rank, n,
+                                              *[a.ctypes.data_as(_vp) for a in arrs],
+                                              ctypes.byref(pos)))
+    return (*arrs, int(pos.value))
+
+
+def read_targets(directory, rank, n, position=0):
+    """n bodies' (pot, ax, ay, az) from <directory>/target%04d.dat: (trg[n, 4], next position)."""
+    t = np.zeros((n, 4))
+    pos = ctypes.c_int64(position)
+    _check_free(lib().tapas_b200_read_targets(_cstr(directory), rank, n, t.ctypes.data_as(_vp),
+                                              ctypes.byref(pos)))
+    return t, int(pos.value)
+
+
+def write_main_csv(path, total, upward, traverse, downward, tree, num_p2p, num_m2l, rank=0):
+    """The example's main.csv row (ex/tapas_exafmm.cxx:651-677) in the reference's layout."""
+    _check_free(lib().tapas_b200_write_main_csv(_cstr(path), rank, total, upward, traverse,
+                                                downward, tree, num_p2p, num_m2l))
 
 
 class Context:
@@ -200,10 +266,20 @@ class Context:
         """Keep the traversal's pairs with empty cells, as the reference does."""
         self._check(self._L.tapas_b200_set_reference_lists(self.h, int(on)))
 
+    def set_wait_limit(self, cycles: int = 0):
+        """Bound (GPU clock cycles) on each wait inside the tensor-core M2L
+        kernel; 0 restores the default (about 2 s)."""
+        self._check(self._L.tapas_b200_set_wait_limit(self.h, int(cycles)))
+
     def timings(self) -> dict:
         t = Timings()
         self._check(self._L.tapas_b200_get_timings(self.h, ctypes.byref(t)))
         return {f: getattr(t, f) for f in _TIMING_FIELDS}
+
+    def write_report(self, prefix=None, suffix=None):
+        """The reference's report files of the last evaluation (main.csv and
+        hot/report.h's set); None: TAPAS_REPORT_PREFIX / _SUFFIX."""
+        self._check(self._L.tapas_b200_write_report(self.h, _cstr(prefix), _cstr(suffix)))
 
     def kernel_launches(self, reset=False) -> int:
         return int(self._L.tapas_b200_kernel_launches(self.h, int(reset)))

@@ -4,7 +4,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
-#include "mixed.cuh"
+#include "m2l_tc.cuh"
 #include "traverse.cuh"
 #include "tree.cuh"
 
@@ -192,7 +192,15 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->op_m2m.release();
   ctx->op_l2l.release();
   ctx->op_part.release();
-  mixed_release(ctx);
+  // mixed-form state: near-field offsets, P2P work items, tensor-core M2L
+  for (auto *b : {&ctx->rel4, &ctx->rel_lo}) b->release();
+  for (auto *b : {&ctx->p2p_wkey, &ctx->p2p_wkey_alt}) b->release();
+  for (auto *b : {&ctx->p2p_order, &ctx->p2p_order_alt}) b->release();
+  for (auto *b : {&ctx->p2p_kcnt, &ctx->p2p_koff, &ctx->p2p_psz, &ctx->p2p_poff}) b->release();
+  ctx->p2p_counter.release();
+  ctx->p2p_items.release();
+  ctx->p2p_part.release();
+  ctx->tc.release();
   mlp_release(ctx);
   ctx->bh_attr.release();
   ctx->bh_attr32.release();
@@ -217,6 +225,12 @@ int tapas_b200_set_profiling(tapas_b200_ctx *ctx, int on) {
 int tapas_b200_set_reference_lists(tapas_b200_ctx *ctx, int on) {
   TB_TRY(check_ctx(ctx));
   ctx->reference_lists = on != 0;  // applies to the next list construction
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_set_wait_limit(tapas_b200_ctx *ctx, int64_t cycles) {
+  TB_TRY(check_ctx(ctx));
+  ctx->tc_wait_limit = cycles > 0 ? (long long)cycles : 4000000000LL;
   return TAPAS_B200_OK;
 }
 
@@ -386,7 +400,7 @@ int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision) {
   ctx->have_M = ctx->have_L = false;
   ctx->P = P;
   ctx->precision = precision;
-  if (precision == TAPAS_B200_MIXED) TB_TRY(upward_mixed(ctx, P));
+  if (precision == TAPAS_B200_MIXED) TB_TRY(upward_fp32_p2m(ctx, P));
   else TB_TRY(upward_fp64(ctx, P));
   ctx->have_M = true;
   return TAPAS_B200_OK;
@@ -394,11 +408,7 @@ int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision) {
 
 int tapas_b200_build_lists(tapas_b200_ctx *ctx, double theta, int mutual) {
   TB_TRY(check_ctx(ctx));
-  if (mutual != 0) {
-    set_error(ctx, "mutual interaction is not supported (as in the reference's CUDA build)");
-    return TAPAS_B200_ERR_UNSUPPORTED;
-  }
-  return build_lists(ctx, theta);
+  return build_lists(ctx, theta, mutual);
 }
 
 int tapas_b200_list_info(tapas_b200_ctx *ctx, tapas_b200_list_stats *out) {
@@ -454,7 +464,7 @@ int tapas_b200_m2l(tapas_b200_ctx *ctx, int precision) {
     return TAPAS_B200_ERR_STATE;
   }
   PhaseTimer t(ctx, &ctx->timings.m2l);
-  if (precision == TAPAS_B200_MIXED) TB_TRY(m2l_mixed(ctx));
+  if (precision == TAPAS_B200_MIXED) TB_TRY(m2l_tensorcore(ctx));
   else TB_TRY(m2l_fp64(ctx));
   ctx->have_L = true;
   return TAPAS_B200_OK;
@@ -487,7 +497,7 @@ int tapas_b200_downward(tapas_b200_ctx *ctx, int precision) {
     return TAPAS_B200_ERR_STATE;
   }
   PhaseTimer t(ctx, &ctx->timings.downward);
-  if (precision == TAPAS_B200_MIXED) return downward_mixed(ctx);
+  if (precision == TAPAS_B200_MIXED) return downward_fp32_l2p(ctx);
   return downward_fp64(ctx);
 }
 
@@ -497,7 +507,6 @@ int tapas_b200_get_expansions(tapas_b200_ctx *ctx, double *M, double *L) {
     set_error(ctx, "get_expansions: no expansions");
     return TAPAS_B200_ERR_STATE;
   }
-  TB_TRY(mixed_sync_fp64_view(ctx));
   const size_t bytes = sizeof(double2) * (size_t)ctx->ncells * nterm_of(ctx->P);
   if (M) TB_CUDA(ctx, cudaMemcpyAsync(M, ctx->M.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (L && ctx->have_L)

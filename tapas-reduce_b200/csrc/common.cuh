@@ -171,7 +171,9 @@ struct tapas_b200_ctx {
   tb::DBuf<int32_t> list_cnt;           // list ordering: per-target counts, cursors, long segments
   tb::DBuf<uint32_t> list_src;          // list ordering: sources grouped by target
   tb::DBuf<unsigned long long> counters; // [next, m2l, p2p, p2p_interactions, overflow]
-  int64_t n_m2l = 0, n_p2p = 0;
+  int64_t n_m2l = 0, n_p2p = 0;         // directed pairs in the lists
+  int64_t n_m2l_visited = 0, n_p2p_visited = 0;  // pairs the traversal emitted (unordered if mutual)
+  int mutual = 0;                       // lists of the last build_lists came from a mutual traversal
   uint64_t n_p2p_int = 0;
   int trav_iters = 0;
   int64_t trav_pairs = 0;  // (target, source) pairs the traversal classified
@@ -200,6 +202,7 @@ struct tapas_b200_ctx {
   int64_t m2l_npairs = 0;
   int64_t tc_classes = 0, tc_tiles = 0, tc_segments = 0, n_m2l_tc = 0;
   size_t tc_op_budget = (size_t)4 << 30;  // bytes of split-TF32 operators kept at once
+  long long tc_wait_limit = 4000000000LL; // clock cycles a tensor-core M2L wait may take
   bool have_M = false, have_L = false;
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
   tb::DBuf<double> op_m2m, op_l2l;      // per level: child<->parent translation operators

@@ -558,12 +558,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // Wait for the phase of `bar` with the given parity; gives up (false) when
-// another role has raised *abort or after about 2 s, then raising *abort.
-__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volatile int *abort) {
+// another role has raised *abort or after `limit` clock cycles (by default
+// 4e9, about 2 s), then raising *abort.
+__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                           long long limit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
     if (*abort) return false;
-    if (clock64() - t0 > 4000000000LL) {
+    if (clock64() - t0 > limit) {
       *abort = 1;
       return false;
     }
@@ -635,7 +637,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
     const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
     const float *__restrict__ ops_lo, const float *__restrict__ Mt_hi,
-    const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err) {
+    const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err,
+    long long wait_limit) {
   using S = TcShape<P>;
   constexpr int NS = S::NS;
   constexpr int NB = S::TBUF;
@@ -716,7 +719,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     int64_t issued = 0;
     for (int64_t step = 0; step < nsteps; step++) {
       const int st = (int)(step % NS);
-      if (step >= NS && !wait_phase(&empty[st], (uint32_t)((step / NS - 1) & 1), abort)) break;
+      if (step >= NS && !wait_phase(&empty[st], (uint32_t)((step / NS - 1) & 1), abort, wait_limit)) break;
       const int64_t jt = step / S::NKC;
       const int kc = (int)(step % S::NKC);
       if (kc == 0) {
@@ -768,14 +771,14 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       for (int64_t jt = 0; jt < ntiles && !*abort; jt++) {
         const int b = NB == 2 ? (int)(jt & 1) : 0;
         const int64_t use_b = NB == 2 ? (jt >> 1) : jt;
-        if (use_b >= 1 && !wait_phase(&tempty[b], (uint32_t)((use_b - 1) & 1), abort)) break;
+        if (use_b >= 1 && !wait_phase(&tempty[b], (uint32_t)((use_b - 1) & 1), abort, wait_limit)) break;
         tc_fence_after();
         const uint32_t dcol = tmem + (uint32_t)(b * S::MT * kNTile);
         bool ok = true;
         for (int kc = 0; kc < S::NKC; kc++) {
           const int64_t step = jt * S::NKC + kc;
           const int st = (int)(step % NS);
-          if (!wait_phase(&full[st], (uint32_t)((step / NS) & 1), abort)) {
+          if (!wait_phase(&full[st], (uint32_t)((step / NS) & 1), abort, wait_limit)) {
             ok = false;
             break;
           }
@@ -822,7 +825,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
 #pragma unroll
       for (int c = 0; c < 2; c++) tg[c] = tg_next[c];
       load_targets(jt + 1, tg_next);
-      if (!wait_phase(&tfull[b], (uint32_t)(use_b & 1), abort)) break;
+      if (!wait_phase(&tfull[b], (uint32_t)(use_b & 1), abort, wait_limit)) break;
       tc_fence_after();
 #pragma unroll 1
       for (int mt = 0; mt < S::MT; mt++) {
@@ -996,7 +999,8 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(it, nitems, T.vals.p, ctx->m2l.p,
                                                         ctx->list_shift, T.ops_hi.p, T.ops_lo.p,
-                                                        mt_hi, mt_lo, T.Lt.p, T.err.p);
+                                                        mt_hi, mt_lo, T.Lt.p, T.err.p,
+                                                        ctx->tc_wait_limit);
     TB_LAUNCH_CHECK(ctx);
   }
   add_scaled_L<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(

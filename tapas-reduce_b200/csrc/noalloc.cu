@@ -138,6 +138,14 @@ extern "C" int tapas_b200_direct_noalloc(const double *x, const double *y, const
     scratch = g_scratch_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // An error left by earlier asynchronous work would otherwise be read back
+  // after the launch below and reported as this call's launch failure.
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(nullptr, "direct_noalloc: a CUDA error from earlier work was pending: %s",
+              cudaGetErrorString(e));
+    return TAPAS_B200_ERR_CUDA;
+  }
   direct_partial<<<dim3((unsigned)k, kSplit), kNoallocThreads, 0, s>>>(x, y, z, q, n, targets,
                                                                        scratch);
   e = cudaGetLastError();

@@ -10,9 +10,18 @@
 //   - a P2P pair    if both are leaves (skipped when either is empty: the
 //                   reference's Map over an empty body product is a no-op,
 //                   cpp/include/tapas/hot.h:1362-1369),
-//   - 8 new pairs   otherwise, splitting by tapas_splitCell (:252-285; with
-//                   mutual = 0: split the non-leaf side, and if both are
-//                   non-leaves the one with the larger R, ties -> target).
+//   - 8 new pairs   otherwise, splitting by tapas_splitCell (:252-285): split
+//                   the non-leaf side, and if both are non-leaves the one with
+//                   the larger R, ties -> target.
+// With mutual = 1 (the example's -m option) a pair (c, c) of a non-leaf cell
+// with itself splits both sides and visits only the 36 child pairs (c_i, c_j),
+// i <= j (tapas_splitCell's `mutual && Ci == Cj` branch; the product map's
+// AllowMutualInteraction rule, cpp/include/tapas/hot/mapper.h:28-121 and
+// iterator.h:98-100,165-167,279-281).  Every unordered cell pair is then
+// visited once and acts both ways (M2L both ways, LaplaceSphericalCPU_tapas.h:
+// 208-273; P2P both ways, LaplaceP2PCPU_tapas.h:48-74).  Here the unordered
+// pairs are expanded into the two directed pairs before the lists are
+// ordered, so the evaluation kernels see ordinary (target, source) lists.
 // The acceptance test is evaluated with separately rounded FP64 operations so
 // every decision matches the reference bit for bit; the lists are therefore
 // equal as sets.  They are then sorted by (target, source) so the evaluation
@@ -58,10 +67,12 @@ __global__ void trav_cells(int64_t ncells, const double *__restrict__ mn,
 }
 
 // Per-thread output counts packed in one word for the block scan: M2L pairs
-// in bits 0-9, P2P pairs in bits 10-19, new frontier pairs in bits 20-31
-// (at most 256, 256 and 8 * 256 per block).
+// in bits 0-8, P2P pairs in bits 9-17, new frontier pairs in bits 18-31
+// (at most 256, 256 and 36 * 256 per block; 36 for a mutual self split).
 constexpr int kWarpsPerBlock = kBlock / 32;
+constexpr int kSelfSplit = 36;  // child pairs (i, j), i <= j, of a cell with itself
 static_assert(kBlock <= 256, "packed per-block counts hold at most 256 threads");
+static_assert(kSelfSplit * kBlock < (1 << 14), "frontier count field is 14 bits");
 
 // counters: [0] next frontier size, [1] m2l size, [2] p2p size,
 //           [3] p2p body-pair interactions, [4] overflow bits (1: a list,
@@ -74,7 +85,7 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
                                                    int64_t m2l_cap, uint64_t *__restrict__ p2p,
                                                    int64_t p2p_cap,
                                                    unsigned long long *__restrict__ counters,
-                                                   int prune_empty) {
+                                                   int prune_empty, int mutual) {
   __shared__ uint32_t wsum[kWarpsPerBlock];
   __shared__ unsigned long long wint[kWarpsPerBlock];
   __shared__ unsigned long long bbase[3];
@@ -82,7 +93,7 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nfront;
        base += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = base + threadIdx.x;
-    int kind = 0;  // 0 none, 1 m2l, 2 p2p, 3 split target, 4 split source
+    int kind = 0;  // 0 none, 1 m2l, 2 p2p, 3 split target, 4 split source, 5 split both
     int t = 0, s = 0, split_child = 0;
     unsigned long long inter = 0;
     if (i < nfront) {
@@ -108,20 +119,25 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
         } else if (lt && ls) {
           if (mt.x > 0 && ms.x > 0) {
             kind = 2;
+            // body pairs evaluated: both directions of a mutual pair of two leaves
             inter = (unsigned long long)mt.x * (unsigned long long)ms.x;
+            if (mutual && t != s) inter *= 2;
           }
         } else if (ls) {
           kind = 3;
         } else if (lt) {
           kind = 4;
+        } else if (mutual && t == s) {
+          kind = 5;
         } else {
           kind = (Ri >= Rj) ? 3 : 4;
         }
         split_child = kind == 3 ? mt.y : ms.y;
       }
     }
-    const uint32_t mine = (kind == 1 ? 1u : 0u) | (kind == 2 ? 1u << 10 : 0u) |
-                          (kind >= 3 ? 8u << 20 : 0u);
+    const uint32_t mine = (kind == 1 ? 1u : 0u) | (kind == 2 ? 1u << 9 : 0u) |
+                          (kind == 3 || kind == 4 ? 8u << 18 : 0u) |
+                          (kind == 5 ? (uint32_t)kSelfSplit << 18 : 0u);
     uint32_t incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -144,7 +160,7 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
         run += v;
         tot += wint[k];
       }
-      const uint32_t n1 = run & 1023u, n2 = (run >> 10) & 1023u, n3 = run >> 20;
+      const uint32_t n1 = run & 511u, n2 = (run >> 9) & 511u, n3 = run >> 18;
       bbase[0] = n1 ? atomicAdd(counters + 1, (unsigned long long)n1) : 0;
       bbase[1] = n2 ? atomicAdd(counters + 2, (unsigned long long)n2) : 0;
       bbase[2] = n3 ? atomicAdd(counters + 0, (unsigned long long)n3) : 0;
@@ -153,17 +169,27 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
     __syncthreads();
     const uint32_t off = wsum[warp] + incl - mine;
     if (kind == 1) {
-      const unsigned long long dst = bbase[0] + (off & 1023u);
+      const unsigned long long dst = bbase[0] + (off & 511u);
       if ((int64_t)dst < m2l_cap) m2l[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
       else atomicOr(counters + 4, 1ull);
     } else if (kind == 2) {
-      const unsigned long long dst = bbase[1] + ((off >> 10) & 1023u);
+      const unsigned long long dst = bbase[1] + ((off >> 9) & 511u);
       if ((int64_t)dst < p2p_cap) p2p[dst] = ((uint64_t)(uint32_t)t << 32) | (uint32_t)s;
       else atomicOr(counters + 4, 1ull);
+    } else if (kind == 5) {
+      const unsigned long long dst = bbase[2] + (off >> 18);
+      if ((int64_t)(dst + kSelfSplit) <= next_cap) {
+        int2 *o = next + dst;
+        int k = 0;
+        for (int a = 0; a < 8; a++)
+          for (int b2 = a; b2 < 8; b2++) o[k++] = make_int2(split_child + a, split_child + b2);
+      } else {
+        atomicOr(counters + 4, 2ull);
+      }
     } else if (kind >= 3) {
-      const unsigned long long dst = bbase[2] + (off >> 20);
+      const unsigned long long dst = bbase[2] + (off >> 18);
       if ((int64_t)(dst + 8) <= next_cap) {
-        int4 *o4 = reinterpret_cast<int4 *>(next + dst);  // dst is a multiple of 8
+        int4 *o4 = reinterpret_cast<int4 *>(next + dst);  // dst is even (8 and 36 are)
         if (kind == 3) {
 #pragma unroll
           for (int k = 0; k < 8; k += 2)
@@ -178,6 +204,39 @@ __global__ void __launch_bounds__(kBlock) dtt_step(TravCells c, const int2 *__re
       }
     }
     __syncthreads();  // wsum / bbase are rewritten by the next round
+  }
+}
+
+// The directed pairs of a mutual list: (t, s) and (s, t) for t != s, a self
+// pair (t, t) once.  Slots are reserved once per warp; the order is set by the
+// (target, source) sort that follows.
+__global__ void expand_mutual(const uint64_t *__restrict__ in, int64_t n,
+                              uint64_t *__restrict__ out, int64_t cap,
+                              unsigned long long *__restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const int64_t i = base + lane;
+    uint64_t x = 0;
+    int k = 0;
+    if (i < n) {
+      x = in[i];
+      k = ((x >> 32) != (x & 0xFFFFFFFFull)) ? 2 : 1;
+    }
+    int incl = k;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long b0 = 0;
+    if (lane == 0) b0 = atomicAdd(cnt, (unsigned long long)tot);
+    b0 = __shfl_sync(0xffffffffu, b0, 0);
+    const int64_t dst = (int64_t)b0 + incl - k;
+    if (k >= 1 && dst < cap) out[dst] = x;
+    if (k == 2 && dst + 1 < cap) out[dst + 1] = (x << 32) | (x >> 32);
   }
 }
 
@@ -321,7 +380,7 @@ int bits_for(int64_t x) {
 
 }  // namespace
 
-int build_lists(tapas_b200_ctx *ctx, double theta) {
+int build_lists(tapas_b200_ctx *ctx, double theta, int mutual) {
   if (!ctx->have_tree) {
     set_error(ctx, "build_lists: no tree (call partition first)");
     return TAPAS_B200_ERR_STATE;
@@ -330,6 +389,11 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
     set_error(ctx, "build_lists: theta must be > 0");
     return TAPAS_B200_ERR_ARG;
   }
+  if (mutual != 0 && mutual != 1) {
+    set_error(ctx, "build_lists: mutual must be 0 or 1");
+    return TAPAS_B200_ERR_ARG;
+  }
+  ctx->mutual = mutual;
   cudaStream_t s = ctx->stream;
   ctx->theta = theta;
   ctx->have_lists = false;
@@ -373,7 +437,7 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
         dtt_step<<<grid_for(nfront, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
             cv, ctx->front_a.p, nfront, ctx->front_b.p, (int64_t)ctx->front_b.cap, ctx->m2l.p,
             (int64_t)ctx->m2l.cap, ctx->p2p.p, (int64_t)ctx->p2p.cap, ctx->counters.p,
-            ctx->reference_lists ? 0 : 1);
+            ctx->reference_lists ? 0 : 1, mutual);
         TB_LAUNCH_CHECK(ctx);
         TB_CUDA(ctx, cudaMemcpyAsync(hc, ctx->counters.p, 5 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, s));
@@ -397,6 +461,29 @@ int build_lists(tapas_b200_ctx *ctx, double theta) {
       if (++iters > 4 * (kMaxDepth + 2)) {
         set_error(ctx, "traversal did not terminate within its iteration bound");
         return TAPAS_B200_ERR_CAPACITY;
+      }
+    }
+    ctx->n_m2l_visited = n_m2l;
+    ctx->n_p2p_visited = n_p2p;
+    if (mutual) {
+      // unordered pairs -> directed pairs (M2L has no self pairs; P2P has one
+      // self pair per non-empty leaf)
+      tb::DBuf<uint64_t> *lists[2] = {&ctx->m2l, &ctx->p2p};
+      int64_t *counts[2] = {&n_m2l, &n_p2p};
+      for (int w = 0; w < 2; w++) {
+        const int64_t n = *counts[w];
+        if (n == 0) continue;
+        TB_CUDA(ctx, ctx->list_alt.ensure(2 * n, s));
+        TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p + 5, 0, sizeof(unsigned long long), s));
+        expand_mutual<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
+            lists[w]->p, n, ctx->list_alt.p, 2 * n, ctx->counters.p + 5);
+        TB_LAUNCH_CHECK(ctx);
+        TB_CUDA(ctx, cudaMemcpyAsync(hc + 5, ctx->counters.p + 5, sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s));
+        TB_CUDA(ctx, cudaStreamSynchronize(s));
+        *counts[w] = (int64_t)hc[5];
+        std::swap(lists[w]->p, ctx->list_alt.p);
+        std::swap(lists[w]->cap, ctx->list_alt.cap);
       }
     }
     ctx->n_m2l = n_m2l;

@@ -15,7 +15,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(p for p in (pathlib.Path(__file__).parent / "golden").glob("*.npz")
-                if not p.stem.startswith("bh_"))
+                if not p.stem.startswith(("bh_", "refsample_", "io_")))
 FP64_RTOL = 1e-11
 
 
@@ -144,12 +144,17 @@ def test_results_fp64(run):
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
 def test_against_reference_goldens(path, tb, ctx):
-    """Directly against outputs of the unmodified reference."""
+    """Directly against outputs of the unmodified reference (with the golden's
+    mutual option: the example's -m)."""
     g = np.load(path)
+    mutual = int(g["mutual"]) if "mutual" in g else 0
     ctx.set_reference_lists(True)
     try:
-        res = ctx.evaluate(g["x"], g["y"], g["z"], g["q"], P=int(g["P"]), ncrit=int(g["ncrit"]),
-                           theta=float(g["theta"]), precision=tb.FP64)
+        ctx.partition(g["x"], g["y"], g["z"], g["q"], ncrit=int(g["ncrit"]))
+        ctx.upward(int(g["P"]), tb.FP64)
+        ctx.traverse(float(g["theta"]), mutual, tb.FP64)
+        ctx.downward(tb.FP64)
+        res = ctx.results(tb.ORDER_ORIGINAL)
     finally:
         ctx.set_reference_lists(False)
     c = ctx.cells()
@@ -158,8 +163,20 @@ def test_against_reference_goldens(path, tb, ctx):
     assert np.array_equal(c["nb"][order], g["cell_nb"])
     assert np.array_equal(c["leaf"][order], g["cell_leaf"])
     li = ctx.list_info()
-    assert li["n_m2l"] == int(g["n_m2l"])
-    assert li["n_p2p_interactions"] == int(g["n_p2p_interactions"])
+    if mutual:
+        # the lists hold both directions of every unordered pair the reference
+        # visited; its counters count visits (j <= i within a leaf)
+        (mt, ms), (pt, ps) = ctx.lists()
+        nb = c["nb"].astype(np.int64)
+        up = pt < ps
+        self_ = pt == ps
+        visits = int(np.sum(nb[pt[up]] * nb[ps[up]]) +
+                     np.sum(nb[pt[self_]] * (nb[pt[self_]] + 1) // 2))
+        assert li["n_m2l"] == 2 * int(g["n_m2l"])
+        assert visits == int(g["n_p2p_interactions"])
+    else:
+        assert li["n_m2l"] == int(g["n_m2l"])
+        assert li["n_p2p_interactions"] == int(g["n_p2p_interactions"])
     assert _rel(res, g["trg"]) < FP64_RTOL
     if "M" in g:
         M, L = ctx.expansions()
@@ -294,8 +311,8 @@ def test_errors_are_status_codes(tb):
         assert e.value.code == -6
         c.upward(6)
         with pytest.raises(tb.TapasError) as e:
-            c.build_lists(0.4, mutual=1)
-        assert e.value.code == -6
+            c.build_lists(0.4, mutual=2)
+        assert e.value.code == -1
         with pytest.raises(tb.TapasError) as e:
             c.downward()
         assert e.value.code == -4
@@ -373,3 +390,52 @@ def test_long_source_lists_are_split(tb, ctx):
     assert num[0] / den[0] < 1e-5 and np.linalg.norm(num[1:]) / np.linalg.norm(den[1:]) < 1e-4
     m = ctx.evaluate(x, y, z, q, P=8, ncrit=64, theta=0.3, precision=tb.MIXED)
     assert np.linalg.norm(m[:, 0] - a[:, 0]) / np.linalg.norm(a[:, 0]) < 2e-6
+
+
+def test_tensorcore_m2l_wait_timeout_is_a_status(tb, ctx):
+    """The tensor-core M2L's designed failure path: with a wait bound of 100
+    clock cycles the MMA thread's first wait for a copy gives up, every role
+    leaves its loop, the CTA drains its copies and MMAs and frees its tensor
+    memory, and the call returns TAPAS_B200_ERR_TIMEOUT.  The same context then
+    evaluates normally with the default bound."""
+    x, y, z, q = tb.datasets.make("plummer", 60000, 61)
+    ctx.partition(x, y, z, q, ncrit=32)
+    ctx.upward(8, tb.FP64)
+    ctx.build_lists(0.4)
+    ctx.m2l(tb.FP64)
+    _, L64 = ctx.expansions()
+    try:
+        ctx.set_wait_limit(100)
+        with pytest.raises(tb.TapasError) as e:
+            ctx.m2l(tb.MIXED)
+        assert e.value.code == tb._lib.ERR_TIMEOUT
+        assert "gave up" in str(e.value)
+    finally:
+        ctx.set_wait_limit(0)
+    ctx.m2l(tb.MIXED)
+    _, Lmx = ctx.expansions()
+    nb = ctx.cells()["nb"]
+    ne = (nb > 0) & (np.linalg.norm(L64, axis=1) > 0)
+    rel = np.linalg.norm(Lmx[ne] - L64[ne], axis=1) / np.linalg.norm(L64[ne], axis=1)
+    assert rel.max() < 2e-5
+
+
+@pytest.mark.parametrize("P", [4, 10, 16])
+@pytest.mark.parametrize("dist", ["sphere_surface", "two_gaussians"])
+def test_fp32_p2m_per_cell(P, dist, tb, ctx):
+    """The mixed form's P2M (FP32 terms in units of the leaf width, FP32 warp
+    reduce-scatter, FP64 sums over body chunks) followed by the FP64 M2M,
+    against the FP64 upward pass, per cell: ||M_mixed - M_fp64|| / ||M_fp64||
+    <= 1e-6.  The sphere-surface set has zero-mean charges (cancelling
+    monopoles); the Gaussian clusters give a deep tree of small cells."""
+    x, y, z, q = tb.datasets.make(dist, 150000, 17)
+    ctx.partition(x, y, z, q, ncrit=32)
+    ctx.upward(P, tb.FP64)
+    M64, _ = ctx.expansions()
+    ctx.upward(P, tb.MIXED)
+    Mmx, _ = ctx.expansions()
+    assert ctx.tree_info()["max_depth"] >= 7
+    nrm = np.linalg.norm(M64, axis=1)
+    ok = nrm > 0
+    rel = np.linalg.norm(Mmx[ok] - M64[ok], axis=1) / nrm[ok]
+    assert rel.max() < 1e-6, (rel.max(), np.median(rel))

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 GOLDEN = sorted(p for p in (pathlib.Path(__file__).parent / "golden").glob("*.npz")
-                if not p.stem.startswith("bh_"))
+                if not p.stem.startswith(("bh_", "refsample_", "io_")))
 BH_GOLDEN = sorted((pathlib.Path(__file__).parent / "golden").glob("bh_*.npz"))
 
 
@@ -27,8 +27,9 @@ def test_bh_oracle_matches_reference(path, oracle_mod):
 @pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
 def test_oracle_matches_reference(path, oracle_mod):
     g = np.load(path)
+    mutual = int(g["mutual"]) if "mutual" in g else 0
     o = oracle_mod.Oracle(g["x"], g["y"], g["z"], g["q"], P=int(g["P"]), ncrit=int(g["ncrit"]),
-                          theta=float(g["theta"]))
+                          theta=float(g["theta"]), mutual=mutual)
     c = o.cells()
     order = np.argsort(c["key"], kind="stable")
     assert np.array_equal(c["key"][order], g["cell_key"])
@@ -59,3 +60,31 @@ def test_oracle_accuracy_vs_direct(oracle_mod):
     d = oracle_mod.direct(x, y, z, q, tg)
     ep, ea = oracle_mod.rel_l2(o.result()[tg], d)
     assert ep < 1e-4 and ea < 1e-3
+
+
+SAMPLED = sorted((pathlib.Path(__file__).parent / "golden").glob("refsample_*.npz"))
+
+
+@pytest.mark.parametrize("path", SAMPLED, ids=[p.stem for p in SAMPLED])
+def test_sampled_fixture_inputs_regenerate(path, tb):
+    """The benchmark-sized fixtures keep only a sample of the reference's
+    results; their inputs are regenerated from the seed, and the generator
+    must still produce the bodies the reference ran on."""
+    g = np.load(path)
+    n = int(g["n"])
+    x, y, z, q = tb.datasets.make(str(g["dist"]), n, int(g["seed"]))
+    w = np.arange(1, n + 1, dtype=np.float64) % 1009.0 + 1.0
+    np.testing.assert_array_equal(np.array([np.dot(w, a) for a in (x, y, z, q)]), g["checksum"])
+    np.testing.assert_array_equal(g["idx"], tb.datasets.sample_targets(n, len(g["idx"]), 1234))
+
+
+def test_oracle_matches_reference_at_100k(tb, oracle_mod):
+    """The restatement against the reference at the 100k-body cube (P=10,
+    theta=0.4, ncrit=64): bit for bit on the sampled bodies, same counters."""
+    g = np.load(pathlib.Path(__file__).parent / "golden" / "refsample_cube_n100000_p10.npz")
+    x, y, z, q = tb.datasets.make(str(g["dist"]), int(g["n"]), int(g["seed"]))
+    o = oracle_mod.Oracle(x, y, z, q, P=int(g["P"]), ncrit=int(g["ncrit"]),
+                          theta=float(g["theta"]))
+    assert len(o.m2l_list()[0]) == int(g["n_m2l"])
+    assert o.p2p_interactions() == int(g["n_p2p_interactions"])
+    np.testing.assert_array_equal(o.result()[g["idx"]], g["trg"])

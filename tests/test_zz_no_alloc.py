@@ -51,6 +51,36 @@ def test_direct_noalloc_matches_direct(tb):
             assert np.all(np.abs(got - ref) <= 1e-12 * scale), call
 
 
+def test_direct_noalloc_bad_index_and_stream(tb):
+    """A target index outside [0, n) gives an all-NaN row (the other rows are
+    unaffected), and the work runs on the caller's stream: results read after
+    synchronising only that stream match the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    L = tb.lib()
+    L.tapas_b200_last_error.restype = ctypes.c_char_p
+    x, y, z, q = tb.datasets.make("uniform_cube", 50_000, 73)
+    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
+    n = len(x)
+    tg = np.array([3, -1, 17, n, 4999], dtype=np.int64)
+    good = np.array([0, 2, 4])
+    with tb.Context(0) as ctx:
+        ctx.partition(x, y, z, q, ncrit=64)
+        ref = ctx.direct(tg[good])
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        tg_d = torch.from_numpy(tg).to("cuda", non_blocking=False)
+        out = torch.zeros((len(tg), 4), dtype=torch.float64, device="cuda")
+    stream.synchronize()
+    rc = _noalloc(L, dev, tg_d, len(tg), out, stream=stream.cuda_stream)
+    assert rc == 0, L.tapas_b200_last_error(None)
+    stream.synchronize()
+    got = out.cpu().numpy()
+    assert np.isnan(got[1]).all() and np.isnan(got[3]).all()
+    scale = np.max(np.abs(ref), axis=0)
+    assert np.all(np.abs(got[good] - ref) <= 1e-12 * scale)
+
+
 def test_direct_noalloc_rejects_too_many_targets(tb):
     torch = pytest.importorskip("torch")
     L = tb.lib()
