@@ -175,7 +175,11 @@ def replica_throughput(pg, ms: float, n: int):
 # reference CPU implementation (oracle/_ref, built from the reference sources)
 # ---------------------------------------------------------------------------
 REF_SAMPLE_N = 50_000
-REF_P, REF_THETA, REF_NCRIT = 12, 0.3, 64
+# The setting the reference runs on its samples: the one the learned chooser
+# picks for the 16M sphere-surface workload (and the sampled reference output
+# of that workload was made with), so both arms evaluate the same method.
+REF_P, REF_THETA, REF_NCRIT = 15, 0.4, 128
+GOLDEN = ROOT / "tests" / "golden"
 
 
 def cpu_reference_run(tb, orc, n=REF_SAMPLE_N, seed=77):
@@ -219,14 +223,28 @@ def cpu_reference_parallel(tb, orc, n, seed, workers):
     return workers * n / slowest, runs[0][1], slowest
 
 
+def reference_scaling_evidence():
+    """Per-particle rate of the reference (1 core, same distribution and
+    setting) at the sizes its sampled outputs were made at: it shows how the
+    bounded-sample rate carries to the full workload."""
+    out = {}
+    for name in ("refsample_sphere_n1000000_p15", "refsample_sphere_n16000000_p15"):
+        f = GOLDEN / f"{name}.npz"
+        if f.exists():
+            g = np.load(f)
+            out[f"n{int(g['n'])}"] = _r(int(g["n"]) / float(g["ref_seconds"]))
+    return out
+
+
 def cpu_baseline_obj(value, kind, secs, n=REF_SAMPLE_N, cores=1):
     who = ("1 rank x 1 thread (the reference's Serial threading)" if cores == 1 else
            f"{cores} concurrent single-thread reference processes, one per host thread, "
            f"each on its own sample of {n} bodies")
     return {"value": value, "unit": "particles/s", "cores": cores, "kind": kind,
             "sample": f"{n} bodies of the same sphere-surface workload, "
-                      f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (meets 1e-6 on it), "
-                      f"{who}, {secs:.2f} s"}
+                      f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (the timed setting), "
+                      f"{who}, {secs:.2f} s",
+            "ref_rate_at_full_sizes_1core": reference_scaling_evidence()}
 
 
 def run_reference_arm(args):
@@ -262,21 +280,103 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _r(v, sig=4):
+    """A float rounded to `sig` significant digits (keeps the JSON line short)."""
+    if v is None or isinstance(v, (bool, int, str)):
+        return v
+    v = float(v)
+    if v == 0 or not np.isfinite(v):
+        return v
+    return float(f"{v:.{sig}g}")
+
+
+def _rr(obj):
+    if isinstance(obj, dict):
+        return {k: _rr(v) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [_rr(v) for v in obj]
+    return _r(obj) if isinstance(obj, float) else obj
+
+
 def choose(tb, n, tol, precision):
     from importlib import import_module
     chooser = import_module("tapas_reduce_b200.chooser")
     return chooser.choose_params(n=n, tol=tol, precision=precision)
 
 
-def time_steps(ctx, fn, steps, warmup, stream_sync):
+def reference_sample(name):
+    """Sampled FP64 output of the unmodified reference on a seeded body set
+    (tests/golden/refsample_*.npz): (indices, values, setting) or None."""
+    f = GOLDEN / f"{name}.npz"
+    if not f.exists():
+        return None
+    g = np.load(f)
+    return g["idx"], g["trg"], (int(g["P"]), float(g["theta"]), int(g["ncrit"]))
+
+
+def rel_l2_pair(a, b):
+    ep = np.linalg.norm(a[:, 0] - b[:, 0]) / np.linalg.norm(b[:, 0])
+    ea = np.linalg.norm(a[:, 1:] - b[:, 1:]) / np.linalg.norm(b[:, 1:])
+    return float(ep), float(ea)
+
+
+def verified(ctx, tb, orc, dev, out_dev, tries, d_check, tg, tol, precision):
+    """The first setting of `tries` whose result meets `tol` against the FP64
+    direct sum on the sampled targets; (setting, tried-and-missed)."""
+    missed = []
+    for cand in tries:
+        cand = dict(cand)
+        try:
+            ctx.evaluate(*dev, P=cand["P"], ncrit=cand["ncrit"], theta=cand["theta"],
+                         precision=precision, out=out_dev)
+            e = orc.rel_l2(out_dev.cpu().numpy()[tg], d_check)[0]
+        except tb.TapasError as err:  # e.g. a setting too large for device memory
+            cand["error"] = str(err)
+            e = float("inf")
+        cand["verified_rel_l2_pot"] = e
+        if e <= tol:
+            return cand, missed
+        missed.append(cand)
+    return None, missed
+
+
+def device_time(torch, stream, step, steps, warmup, pg, clocks=None):
+    """CUDA-event milliseconds per step on `stream` (max over ranks), after
+    `warmup` untimed steps, bracketed by barriers and synchronisations."""
     for _ in range(warmup):
-        fn()
-    stream_sync()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        fn()
-    stream_sync()
-    return (time.perf_counter() - t0) / steps
+        step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.__enter__()
+    try:
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    finally:
+        if clocks is not None:
+            clocks.__exit__(None, None, None)
+    barrier(pg)
+    return max_over_ranks(pg, ev0.elapsed_time(ev1) / steps)
+
+
+def profiled_phases(ctx, step):
+    """Phase times (ms) of one extra, untimed step with per-phase events."""
+    ctx.set_profiling(True)
+    try:
+        step()
+        return ctx.timings()
+    finally:
+        ctx.set_profiling(False)
+
+
+def phases_compact(ph):
+    keys = ("bbox_keys", "sort", "tree", "p2m", "m2m", "traverse", "list_sort", "m2l_setup",
+            "m2l_tc", "m2l_fp64", "m2l", "p2p", "l2l", "l2p", "download")
+    return {k: _r(ph.get(k, 0.0)) for k in keys if ph.get(k, 0.0) > 0}
 
 
 def main():
@@ -295,8 +395,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the other configurations (100k cube vs the reference, 1M "
-                         "Plummer, 4M Barnes-Hut)")
+                    help="skip the other configurations (100k cube, 1M Plummer, 1M sphere, "
+                         "4M Barnes-Hut)")
     ap.add_argument("--ref-sample", type=int, default=REF_SAMPLE_N,
                     help="bodies per reference CPU step (--impl reference)")
     ap.add_argument("--ref-threads", type=int, default=0,
@@ -311,7 +411,8 @@ def main():
     torch.cuda.set_device(local)
     tb = load_package()
     n = args.n
-    x, y, z, q = tb.datasets.make(WORKLOAD, n, seed=5 + 1000 * rank)
+    seed = 5 + 1000 * rank
+    x, y, z, q = tb.datasets.make(WORKLOAD, n, seed=seed)
     tg = tb.datasets.sample_targets(n, args.targets, seed=99 + rank)
     dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
     pinned = [torch.from_numpy(a).pin_memory() for a in (x, y, z, q)]
@@ -327,6 +428,7 @@ def main():
     # table's setting is used instead.
     from importlib import import_module
     chooser = import_module("tapas_reduce_b200.chooser")
+    feats = None
     if args.P and args.theta and args.ncrit:
         # fixed setting (profiling a given configuration); still verified
         tries = [{"P": args.P, "theta": args.theta, "ncrit": args.ncrit, "precision": "mixed",
@@ -338,25 +440,12 @@ def main():
         feats = chooser.system_features(ctx, *dev)
         tries = chooser.candidates(ctx, feats, n, args.tol, "mixed", k=3)
     d_check = ctx.direct(tg)
-    prm, tried = None, []
-    for cand in tries:
-        cand = dict(cand)
-        try:
-            ctx.evaluate(*dev, P=cand["P"], ncrit=cand["ncrit"], theta=cand["theta"],
-                         precision=tb.MIXED, out=out_dev)
-            e_check = orc.rel_l2(out_dev.cpu().numpy()[tg], d_check)[0]
-        except tb.TapasError as err:  # e.g. a setting too large for device memory
-            cand["error"] = str(err)
-            e_check = float("inf")
-        cand["verified_rel_l2_pot"] = e_check
-        if e_check <= args.tol:
-            prm = cand
-            break
-        tried.append(cand)
+    prm, missed = verified(ctx, tb, orc, dev, out_dev, tries, d_check, tg, args.tol, tb.MIXED)
     if prm is None:  # no candidate verified: the rule table's setting
         prm = choose(tb, n, args.tol, "mixed")
-    if tried:
-        prm["missed_before"] = tried
+    if missed:
+        prm["missed_before"] = [{k: _r(v) for k, v in m.items() if k in
+                                 ("P", "theta", "ncrit", "verified_rel_l2_pot")} for m in missed]
     P, theta, ncrit = prm["P"], prm["theta"], prm["ncrit"]
     torch.cuda.synchronize()
 
@@ -366,74 +455,79 @@ def main():
     def step_e2e():
         ctx.evaluate(*pinned, P=P, ncrit=ncrit, theta=theta, precision=tb.MIXED, out=out_pin)
 
-    sync = stream.synchronize
     # ---- timed region: device-resident inputs, CUDA events on our stream ----
+    ctx.set_profiling(False)
     for _ in range(args.warmup):
         step_dev()
-    ctx.set_profiling(True)
     ctx.kernel_launches(reset=True)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    phase_acc = {}
-    barrier(pg)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step_dev()
-            for k, v in ctx.timings().items():
-                phase_acc[k] = phase_acc.get(k, 0.0) + v
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier(pg)
-    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = ClockSampler(local)
+    ms_max = device_time(torch, stream, step_dev, args.steps, 0, pg, clocks=clk)
     launches = ctx.kernel_launches() // args.steps
-    ctx.set_profiling(False)
     clocks = clk.summary()
-    ms_max, n_total, value = replica_throughput(pg, ms, n)
-    phases = {k: v / args.steps for k, v in phase_acc.items()}
+    _, n_total, value = replica_throughput(pg, ms_max, n)
+    phases = profiled_phases(ctx, step_dev)  # one extra step with phase events
     li = ctx.list_info()
     ti = ctx.tree_info()
 
-    # ---- verification against FP64 direct sum on sampled targets ----
+    # ---- accuracy: FP64 direct sum on sampled targets, reference's output ----
     res = out_dev.cpu().numpy()
-    d = ctx.direct(tg)
-    err = orc.rel_l2(res[tg], d)
+    err = orc.rel_l2(res[tg], d_check)
+    accuracy = {"rel_l2_pot": _r(err[0]), "rel_l2_acc": _r(err[1]), "targets": int(len(tg)),
+                "meets_tol": bool(err[0] <= args.tol)}
+    ref16 = reference_sample("refsample_sphere_n16000000_p15") if (n == 16_000_000 and
+                                                                     rank == 0) else None
+    if ref16 is not None and ref16[2] == (P, theta, ncrit):
+        e = rel_l2_pair(res[ref16[0]], ref16[1])
+        accuracy.update(rel_l2_pot_vs_reference=_r(e[0]), rel_l2_acc_vs_reference=_r(e[1]),
+                        reference_samples=int(len(ref16[0])))
 
-    # ---- e2e through the C-ABI call with pinned host buffers ----
+    # ---- e2e through the C-ABI call with pinned host buffers, K steps ----
     for _ in range(2):
         step_e2e()
     barrier(pg)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e_steps = max(1, min(args.steps, 3))
-    for _ in range(e_steps):
+    for _ in range(args.steps):
         step_e2e()
-    e2e_s = (time.perf_counter() - t0) / e_steps
-    e2e_s = max_over_ranks(pg, e2e_s)
-    e2e = {"value": n_total / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 4 * 8 * n,
-           "d2h_bytes_per_step": 4 * 8 * n}
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(pg, (time.perf_counter() - t0) / args.steps)
+    e2e = {"value": _r(n_total / e2e_s), "unit": "particles/s",
+           "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n}
 
-    # ---- plain FP64 form at the same tolerance rule ----
+    # ---- plain FP64 form: at the mixed arm's setting, and its own learned choice ----
     fp64 = None
     if not args.no_fp64:
-        p64 = choose(tb, n, args.tol, "fp64")
-
-        def step64():
-            ctx.evaluate(*dev, P=p64["P"], ncrit=p64["ncrit"], theta=p64["theta"],
-                         precision=tb.FP64, out=out_dev)
-        step64()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(2):
-            step64()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms64 = max_over_ranks(pg, e0.elapsed_time(e1) / 2)
-        err64 = orc.rel_l2(out_dev.cpu().numpy()[tg], d)
-        fp64 = {"value": n_total / (ms64 * 1e-3), "unit": "particles/s", "ms_per_step": ms64,
-                "params": p64, "rel_l2_pot": err64[0], "rel_l2_acc": err64[1],
-                "mixed_speedup": ms64 / ms_max}
+        fp64 = {}
+        settings = [("same_setting", {"P": P, "theta": theta, "ncrit": ncrit,
+                                      "source": "the mixed arm's setting"})]
+        if feats is not None:
+            c64, missed64 = verified(ctx, tb, orc, dev, out_dev,
+                                     chooser.candidates(ctx, feats, n, args.tol, "fp64", k=3),
+                                     d_check, tg, args.tol, tb.FP64)
+            if c64 is not None:
+                settings.append(("learned_fp64", c64))
+        for key, s64 in settings:
+            def step64(s64=s64):
+                ctx.evaluate(*dev, P=s64["P"], ncrit=s64["ncrit"], theta=s64["theta"],
+                             precision=tb.FP64, out=out_dev)
+            ms64 = device_time(torch, stream, step64, 2, 1, pg)
+            e64 = orc.rel_l2(out_dev.cpu().numpy()[tg], d_check)
+            ph64 = profiled_phases(ctx, step64)
+            li64, ti64 = ctx.list_info(), ctx.tree_info()
+            rl64 = roofline_obj(ph64, li64, ti64, s64["P"], tb, precision="fp64")
+            fp64[key] = {"ms_per_step": _r(ms64), "value": _r(n_total / (ms64 * 1e-3)),
+                         "P": s64["P"], "theta": s64["theta"], "ncrit": s64["ncrit"],
+                         "rel_l2_pot": _r(e64[0]), "rel_l2_acc": _r(e64[1]),
+                         "meets_tol": bool(e64[0] <= args.tol),
+                         "phases_ms": phases_compact(ph64),
+                         "roofline": {k: _r(v) for k, v in rl64.items()
+                                      if k in ("kernel", "ms", "bound", "achieved", "peak",
+                                               "unit", "frac")},
+                         "work": {"n_m2l": li64["n_m2l"],
+                                  "n_p2p_interactions": li64["n_p2p_interactions"]}}
+        ok = [v["ms_per_step"] for v in fp64.values() if v["meets_tol"]]
+        if ok:
+            fp64["mixed_speedup_vs_fastest_fp64_meeting_tol"] = _r(min(ok) / ms_max)
 
     # ---- roofline of the dominant kernel ----
     roofline = roofline_obj(phases, li, ti, P, tb)
@@ -447,11 +541,12 @@ def main():
     if rank == 0 and not args.no_configs:
         configs = {}
         for key, fn in (("cube_1e5", config_cube_100k), ("plummer_1e6", config_plummer_1m),
+                        ("sphere_1e6_p15", config_sphere_1m),
                         ("barnes_hut_plummer_4e6", config_bh_4m)):
             try:
-                configs[key] = fn(tb, orc, ctx, torch, stream)
+                configs[key] = _rr(fn(tb, orc, ctx, torch, stream))
             except Exception as err:  # reported, never fatal to the headline line
-                configs[key] = {"error": str(err)}
+                configs[key] = {"error": str(err)[:200]}
             torch.cuda.empty_cache()
 
     if rank == 0:
@@ -461,19 +556,17 @@ def main():
                 "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": f"{WORKLOAD} N={n} q=U[-1,1]-mean tol={args.tol}",
                            "bodies_per_gpu": n, "P": P, "theta": theta, "ncrit": ncrit,
-                           "chooser": {k: v for k, v in prm.items()
+                           "chooser": {k: _r(v) for k, v in prm.items()
                                        if k not in ("P", "theta", "ncrit")},
                            "precision": "mixed",
                            "l2_flush": "inputs larger than L2 (512 MB of bodies per step)",
                            "parallelism": f"replicas x{world}"},
-                "accuracy": {"rel_l2_pot": err[0], "rel_l2_acc": err[1],
-                             "targets": int(len(tg)), "meets_tol": bool(err[0] <= args.tol)},
-                "e2e": e2e, "fp64": fp64, "phases_ms": phases,
+                "accuracy": accuracy, "e2e": e2e, "fp64": fp64,
+                "phases_ms": phases_compact(phases),
                 "work": {"n_m2l": li["n_m2l"], "n_p2p_interactions": li["n_p2p_interactions"],
                          "n_cells": ti["n_cells"], "max_depth": ti["max_depth"]},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "configs": configs,
-                "gpu_launches": launches}
+                "roofline": _rr(roofline), "cpu_baseline": cpu, "clocks": clocks,
+                "configs": configs, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg is not None:
@@ -502,58 +595,55 @@ def _rel(a, b):
     return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
 
 
-def config_cube_100k(tb, orc, ctx, torch, stream):
-    """100,000 bodies uniform in [-1,1]^3, charges U[0,1] summing to 1, P=10,
-    theta=0.4, ncrit=64: both forms against the FP64 direct sum on 1,000
-    targets and against the reference's own FP64 output on the same bodies."""
-    n = 100_000
-    x, y, z, q = tb.datasets.make("uniform_cube", n, 101)
+def _fmm_config(tb, ctx, torch, stream, dist, n, seed, P, ncrit, theta, ntarg, tseed, refname):
+    """Both forms at one setting: CUDA-event time, rel-L2 against the FP64
+    direct sum on sampled targets and against the reference's own FP64 output
+    on its sampled bodies (tests/golden/refsample_*)."""
+    x, y, z, q = tb.datasets.make(dist, n, seed)
     dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
     out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
-    tg = tb.datasets.sample_targets(n, 1000, seed=7)
-    res = {"workload": "uniform cube N=1e5 q=U[0,1]/sum P=10 theta=0.4 ncrit=64"}
-    ref = None
-    if orc.reference_available(10):
-        R = orc.run_reference(x, y, z, q, P=10, ncrit=64, theta=0.4)
-        b = R["bodies"]
-        ref = np.empty((n, 4))
-        ref[b["ibody"]] = b["trg"]
-        t = R["times"]
-        res["reference_cpu_1core_ms"] = 1e3 * (t["tree"] + t["upward"] + t["traverse"] + t["downward"])
+    tg = tb.datasets.sample_targets(n, ntarg, seed=tseed)
+    ref = reference_sample(refname)
+    res = {"workload": f"{dist} N={n} P={P} theta={theta} ncrit={ncrit}"}
+    if ref is not None:
+        gf = np.load(GOLDEN / f"{refname}.npz")
+        res["reference_1core_s"] = float(gf["ref_seconds"])
     for prec, name in ((tb.FP64, "fp64"), (tb.MIXED, "mixed")):
-        ms = _timed(torch, stream, lambda: ctx.evaluate(*dev, P=10, ncrit=64, theta=0.4,
+        ms = _timed(torch, stream, lambda: ctx.evaluate(*dev, P=P, ncrit=ncrit, theta=theta,
                                                          precision=prec, out=out))
         r = out.cpu().numpy()
         d = ctx.direct(tg)
-        e = {"ms": ms, "rel_l2_pot_vs_direct": _rel(r[tg, 0], d[:, 0]),
+        e = {"ms": ms, "particles_per_s": n / (ms * 1e-3),
+             "rel_l2_pot_vs_direct": _rel(r[tg, 0], d[:, 0]),
              "rel_l2_acc_vs_direct": _rel(r[tg, 1:], d[:, 1:])}
-        if ref is not None:
-            e["rel_l2_pot_vs_reference"] = _rel(r[:, 0], ref[:, 0])
-            e["rel_l2_acc_vs_reference"] = _rel(r[:, 1:], ref[:, 1:])
+        if ref is not None and ref[2] == (P, theta, ncrit):
+            ep, ea = rel_l2_pair(r[ref[0]], ref[1])
+            e["rel_l2_pot_vs_reference"] = ep
+            e["rel_l2_acc_vs_reference"] = ea
         res[name] = e
+    res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
     return res
+
+
+def config_cube_100k(tb, orc, ctx, torch, stream):
+    """100,000 bodies uniform in [-1,1]^3, charges U[0,1] summing to 1, P=10,
+    theta=0.4, ncrit=64 (the reference's CPU-runnable configuration)."""
+    return _fmm_config(tb, ctx, torch, stream, "uniform_cube", 100_000, 101, 10, 64, 0.4, 1000,
+                       7, "refsample_cube_n100000_p10")
 
 
 def config_plummer_1m(tb, orc, ctx, torch, stream):
     """1M Plummer bodies (scale radius 1, r < 100), charges 1/N, P=10,
-    theta=0.4, ncrit=64: plain FP64 against the mixed form, errors against the
-    FP64 direct sum on 2,000 targets."""
-    n = 1_000_000
-    x, y, z, q = tb.datasets.make("plummer", n, 102)
-    dev = [torch.from_numpy(a).cuda() for a in (x, y, z, q)]
-    out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
-    tg = tb.datasets.sample_targets(n, 2000, seed=8)
-    res = {"workload": "Plummer N=1e6 q=1/N P=10 theta=0.4 ncrit=64"}
-    for prec, name in ((tb.FP64, "fp64"), (tb.MIXED, "mixed")):
-        ms = _timed(torch, stream, lambda: ctx.evaluate(*dev, P=10, ncrit=64, theta=0.4,
-                                                         precision=prec, out=out))
-        r = out.cpu().numpy()
-        d = ctx.direct(tg)
-        res[name] = {"ms": ms, "particles_per_s": n / (ms * 1e-3),
-                     "rel_l2_pot_vs_direct": _rel(r[tg, 0], d[:, 0]),
-                     "rel_l2_acc_vs_direct": _rel(r[tg, 1:], d[:, 1:])}
-    res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
-    return res
+    theta=0.4, ncrit=64: plain FP64 against the mixed form."""
+    return _fmm_config(tb, ctx, torch, stream, "plummer", 1_000_000, 102, 10, 64, 0.4, 2000, 8,
+                       "refsample_plummer_n1000000_p10")
+
+
+def config_sphere_1m(tb, orc, ctx, torch, stream):
+    """1M sphere-surface bodies (the headline's distribution), zero-mean
+    charges, at the headline's setting P=15, theta=0.4, ncrit=128."""
+    return _fmm_config(tb, ctx, torch, stream, "sphere_surface", 1_000_000, 104, 15, 128, 0.4,
+                       4000, 10, "refsample_sphere_n1000000_p15")
 
 
 def config_bh_4m(tb, orc, ctx, torch, stream):
@@ -607,12 +697,12 @@ def _peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def roofline_obj(phases, li, ti, P, tb):
+def roofline_obj(phases, li, ti, P, tb, precision="mixed"):
     """Dominant kernel of the step and its roofline."""
     peaks, src = _peaks()
     from importlib import import_module
     rl = import_module("tapas_reduce_b200.roofline")
-    return rl.dominant(phases, li, ti, P, peaks, src)
+    return rl.dominant(phases, li, ti, P, peaks, src, precision=precision)
 
 
 if __name__ == "__main__":

@@ -225,6 +225,36 @@ int tapas_b200_p2p(tapas_b200_ctx *ctx, int precision);
  * (:275-307) for every non-empty leaf. */
 int tapas_b200_downward(tapas_b200_ctx *ctx, int precision);
 
+/* ---- sharded evaluation over several GPUs -------------------------------- */
+/* The reference splits the work over MPI ranks by Morton-key ranges and builds
+ * a locally essential tree per rank (cpp/include/tapas/hot/buildtree.h:
+ * 162-324,461-483, hot/exact_let.h:675-1247).  Here every GPU builds the same
+ * tree from all bodies (the partition is deterministic) and evaluates the
+ * targets it owns; the caller's collectives do the rest (see
+ * tapas-reduce_b200/sharded.py: one all-reduce of the leaves' multipoles
+ * between p2m and m2m, one of the results).  No counterpart call in the
+ * reference.
+ * mask: one byte per cell (get_cells order) of the current tree; bit 0 = this
+ * context computes the cell's local expansion (its M2L list and L2L), bit 1
+ * = it evaluates the cell's bodies (P2M, P2P, L2P).  The owner of a leaf's
+ * bodies must also own the local expansions of the leaf and its ancestors.
+ * NULL clears the mask; a partition clears it too.  With a mask:
+ *  - p2m computes the owned leaves' multipoles (the rest are zero);
+ *  - m2l and p2p evaluate owned targets only; the classification of M2L
+ *    pairs still sees every pair, so each target's arithmetic, and result,
+ *    is the same as without a mask;
+ *  - results of bodies not owned are exactly zero. */
+int tapas_b200_set_owned_cells(tapas_b200_ctx *ctx, const uint8_t *mask, int mem);
+/* The two halves of tapas_b200_upward: P2M of the leaves (M zeroed first),
+ * then M2M of the whole tree from the leaves' multipoles. */
+int tapas_b200_p2m(tapas_b200_ctx *ctx, int P, int precision);
+int tapas_b200_m2m(tapas_b200_ctx *ctx);
+/* Multipoles, ncells x P(P+1)/2 complex FP64 as interleaved (re, im), in host
+ * or device memory (mem): read after p2m or upward, write between p2m and m2m
+ * (or before traverse). */
+int tapas_b200_get_multipoles(tapas_b200_ctx *ctx, double *M, int mem);
+int tapas_b200_set_multipoles(tapas_b200_ctx *ctx, const double *M, int mem);
+
 /* Multipole / local expansions, ncells x P(P+1)/2 complex FP64 values as
  * interleaved (re, im), cells in get_cells order.  Host memory; either may be NULL. */
 int tapas_b200_get_expansions(tapas_b200_ctx *ctx, double *M, double *L);

@@ -127,6 +127,8 @@ struct oracle_fmm {
   int P, nterm, ncrit;
   double theta;
   int mutual;                     /* the example's -m option (0 or 1) */
+  uint8_t *own;                   /* sharded evaluation: per cell bit 0 = local
+                                     expansion computed here, bit 1 = bodies; NULL = all */
   double *x, *y, *z, *q;          /* original order */
   double *sx, *sy, *sz, *sq;      /* sorted order */
   int64_t *perm;                  /* sorted position -> original index */
@@ -168,7 +170,7 @@ void oracle_destroy(oracle_fmm *h) {
   free(h->sx); free(h->sy); free(h->sz); free(h->sq);
   free(h->perm); free(h->skeys); free(h->trg); free(h->cells);
   free(h->M); free(h->L); free(h->m2l_t); free(h->m2l_s); free(h->p2p_t); free(h->p2p_s);
-  free(h->ynm); free(h->ynmt);
+  free(h->ynm); free(h->ynmt); free(h->own);
   free(h);
 }
 
@@ -488,6 +490,50 @@ int oracle_upward(oracle_fmm *h) {
   return 0;
 }
 
+/* ---------------------------------------------------------------------------
+ * Sharded evaluation, restated for the CPU test of the multi-GPU driver
+ * (tapas-reduce_b200/sharded.py): an ownership mask (bit 0: the cell's local
+ * expansion is computed here, bit 1: its bodies are), the upward pass in two
+ * halves with the multipoles exchanged between them, and M2L / P2P / L2L /
+ * L2P restricted to owned targets.  P2M and M2M are per-cell functions of
+ * their inputs, so the halves reproduce oracle_upward exactly.
+ * ------------------------------------------------------------------------- */
+void oracle_set_owned(oracle_fmm *h, const uint8_t *mask) {
+  free(h->own);
+  h->own = NULL;
+  if (mask) {
+    h->own = malloc((size_t)h->ncells);
+    memcpy(h->own, mask, (size_t)h->ncells);
+  }
+}
+
+static void m2m_rec(oracle_fmm *h, int32_t ci) {
+  if (h->cells[ci].leaf) return;
+  for (int i = 0; i < 8; i++) m2m_rec(h, h->cells[ci].child[i]);
+  m2m(h, ci);
+}
+
+int oracle_p2m_only(oracle_fmm *h) {
+  if (!h->cells) return -1;
+  memset(h->M, 0, sizeof(cplx) * (size_t)h->ncells * h->nterm);
+  memset(h->L, 0, sizeof(cplx) * (size_t)h->ncells * h->nterm);
+  for (int64_t c = 0; c < h->ncells; c++)
+    if (h->cells[c].leaf && (!h->own || (h->own[c] & 2))) p2m(h, (int32_t)c);
+  return 0;
+}
+
+int oracle_m2m_only(oracle_fmm *h) {
+  if (!h->cells) return -1;
+  m2m_rec(h, 0);
+  return 0;
+}
+
+void oracle_set_theta(oracle_fmm *h, double theta) { h->theta = theta; }
+
+void oracle_set_multipoles(oracle_fmm *h, const double *M) {
+  memcpy(h->M, M, sizeof(cplx) * (size_t)h->ncells * h->nterm);
+}
+
 /* M2L, :208-273.  With mutual the same call also translates Ci's multipole
  * into Cj's local expansion, from the harmonics at (rho, alpha + pi, beta)
  * (:222-223), accumulated in the same loop (:244-263). */
@@ -631,7 +677,7 @@ static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
   Rj = (Rj / 2 * 1.00001) / h->theta;
   if (R2 > (Ri + Rj) * (Ri + Rj)) {
     push_pair(&h->m2l_t, &h->m2l_s, &h->nm2l, &h->cm2l, ti, si);
-    m2l(h, ti, si);
+    if (!h->own || (h->own[ti] & 1)) m2l(h, ti, si);
   } else if (Ci->leaf && Cj->leaf) {
     /* tapas::Map over an empty body product is skipped (hot.h:1362-1369). */
     if (Ci->nb > 0 && Cj->nb > 0) {
@@ -640,7 +686,7 @@ static void dtt(oracle_fmm *h, int32_t ti, int32_t si) {
        * leaf under mutual */
       h->np2p_int += (h->mutual && ti == si) ? (uint64_t)(Ci->nb * (Ci->nb + 1) / 2)
                                               : (uint64_t)(Ci->nb * Cj->nb);
-      p2p(h, ti, si);
+      if (!h->own || (h->own[ti] & 2)) p2p(h, ti, si);
     }
   } else {
     /* tapas_splitCell, :252-285 (ties split Ci). */
@@ -752,9 +798,12 @@ static void l2p(oracle_fmm *h, int32_t ci) {
 
 /* FMM_Downward, ex/tapas_exafmm.cxx:124-140 */
 static void downward_rec(oracle_fmm *h, int32_t ci) {
+  /* sharded: a cell whose local expansion is computed elsewhere has no owned
+   * descendant either (owners of bodies own all their ancestors) */
+  if (h->own && !(h->own[ci] & 1)) return;
   if (ci != 0) l2l(h, ci);
   if (h->cells[ci].leaf) {
-    if (h->cells[ci].nb > 0) l2p(h, ci);
+    if (h->cells[ci].nb > 0 && (!h->own || (h->own[ci] & 2))) l2p(h, ci);
   } else {
     for (int i = 0; i < 8; i++) downward_rec(h, h->cells[ci].child[i]);
   }

@@ -37,6 +37,17 @@ int oracle_traverse(oracle_fmm *h);  /* dual-tree traversal: M2L + P2P     */
 /* The example's -m option: mutual = 1 visits each unordered cell pair once
  * and applies M2L and P2P both ways (set before oracle_traverse). */
 void oracle_set_mutual(oracle_fmm *h, int mutual);
+
+/* Sharded evaluation (mutual = 0): per-cell ownership bytes in this oracle's
+ * cell order (bit 0: local expansion computed here, bit 1: bodies), NULL for
+ * all; the upward pass in two halves with the multipoles settable between
+ * them; oracle_traverse / oracle_downward then evaluate owned targets only
+ * (the other bodies' results stay 0). */
+void oracle_set_owned(oracle_fmm *h, const uint8_t *mask);
+int oracle_p2m_only(oracle_fmm *h);
+int oracle_m2m_only(oracle_fmm *h);
+void oracle_set_multipoles(oracle_fmm *h, const double *M);
+void oracle_set_theta(oracle_fmm *h, double theta);
 int oracle_downward(oracle_fmm *h);  /* L2L + L2P                          */
 int oracle_run_all(oracle_fmm *h);
 

@@ -62,6 +62,15 @@ def lib():
         L.oracle_destroy.argtypes = [_vp]
         L.oracle_set_mutual.argtypes = [_vp, ctypes.c_int]
         L.oracle_set_mutual.restype = None
+        L.oracle_set_owned.argtypes = [_vp, _vp]
+        L.oracle_set_owned.restype = None
+        for f in ("oracle_p2m_only", "oracle_m2m_only"):
+            getattr(L, f).argtypes = [_vp]
+            getattr(L, f).restype = ctypes.c_int
+        L.oracle_set_multipoles.argtypes = [_vp, _vp]
+        L.oracle_set_multipoles.restype = None
+        L.oracle_set_theta.argtypes = [_vp, ctypes.c_double]
+        L.oracle_set_theta.restype = None
         for f in ("oracle_ncells", "oracle_n_m2l", "oracle_n_p2p"):
             getattr(L, f).argtypes = [_vp]
             getattr(L, f).restype = _c_i64
@@ -178,6 +187,75 @@ class Oracle:
         o, _, t = self.bodies()
         out = np.empty_like(t)
         out[o] = t
+        return out
+
+
+class OracleContext:
+    """The methods of the library's Context that the sharded driver
+    (tapas-reduce_b200/sharded.py) calls, carried out by the oracle: the CPU
+    stand-in for one GPU in the multi-process (gloo) test of that driver.
+    FP64 form, mutual = 0."""
+
+    def __init__(self):
+        self.o = None
+        self._mask = None
+
+    def partition(self, x, y, z, q, ncrit=64):
+        self._bodies = [np.ascontiguousarray(np.asarray(a), dtype=np.float64) for a in (x, y, z, q)]
+        self.ncrit = ncrit
+        self._new(P=2)
+
+    def _new(self, P):
+        self.o = Oracle(*self._bodies, P=P, ncrit=self.ncrit, theta=0.4, run=False)
+        if lib().oracle_build(self.o.h):
+            raise RuntimeError("oracle_build failed")
+        if self._mask is not None:
+            lib().oracle_set_owned(self.o.h, _p(self._mask))
+
+    def tree_info(self):
+        return {"n_cells": int(lib().oracle_ncells(self.o.h))}
+
+    def cells(self):
+        d = self.o.cells()
+        d["bbeg"] = d["bid"]
+        return d
+
+    def set_owned_cells(self, mask):
+        self._mask = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        lib().oracle_set_owned(self.o.h, None if mask is None else _p(self._mask))
+
+    def p2m(self, P=10, precision=0):
+        self._new(P)
+        lib().oracle_p2m_only(self.o.h)
+
+    def multipoles(self, out=None):
+        M, _ = self.o.expansions()
+        flat = np.stack([M.real, M.imag], axis=-1).reshape(-1)
+        if out is None:
+            return M
+        out.reshape(-1)[:] = flat
+        return out
+
+    def set_multipoles(self, M):
+        lib().oracle_set_multipoles(self.o.h, _p(np.ascontiguousarray(M, dtype=np.float64)))
+
+    def m2m(self):
+        lib().oracle_m2m_only(self.o.h)
+
+    def traverse(self, theta=0.4, mutual=0, precision=0):
+        if mutual:
+            raise ValueError("the oracle's sharded restatement covers mutual = 0")
+        lib().oracle_set_theta(self.o.h, float(theta))
+        lib().oracle_traverse(self.o.h)
+
+    def downward(self, precision=0):
+        lib().oracle_downward(self.o.h)
+
+    def results(self, order=1, out=None):
+        r = self.o.result()
+        if out is None:
+            return r
+        out[...] = r
         return out
 
 

@@ -37,6 +37,8 @@ EXPORTS = (
     "tapas_b200_bh_counts", "tapas_b200_bh_evaluate",
     "tapas_b200_write_sources", "tapas_b200_write_targets", "tapas_b200_read_sources",
     "tapas_b200_read_targets", "tapas_b200_write_main_csv", "tapas_b200_write_report",
+    "tapas_b200_set_owned_cells", "tapas_b200_p2m", "tapas_b200_m2m",
+    "tapas_b200_get_multipoles", "tapas_b200_set_multipoles",
 )
 
 
@@ -140,6 +142,11 @@ def lib():
         "tapas_b200_write_main_csv": [_cp, _int, _dbl, _dbl, _dbl, _dbl, _dbl,
                                       ctypes.c_uint64, ctypes.c_uint64],
         "tapas_b200_write_report": [_vp, _cp, _cp],
+        "tapas_b200_set_owned_cells": [_vp, _vp, _int],
+        "tapas_b200_p2m": [_vp, _int, _int],
+        "tapas_b200_m2m": [_vp],
+        "tapas_b200_get_multipoles": [_vp, _vp, _int],
+        "tapas_b200_set_multipoles": [_vp, _vp, _int],
     })
     for name, args in sig2.items():
         f = getattr(L, name)
@@ -322,6 +329,45 @@ class Context:
     def upward(self, P: int = 10, precision: int = FP64):
         self.P = P
         self._check(self._L.tapas_b200_upward(self.h, P, precision))
+
+    # ---- sharded evaluation (tapas-reduce_b200/sharded.py) ---------------
+    def set_owned_cells(self, mask):
+        """Per-cell ownership bytes (bit 0: local expansion, bit 1: bodies) of
+        the current tree; None clears."""
+        if mask is None:
+            self._check(self._L.tapas_b200_set_owned_cells(self.h, None, HOST))
+            return
+        if isinstance(mask, np.ndarray):
+            mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        p, mem = _ptr(mask)
+        self._keep_mask = mask
+        self._check(self._L.tapas_b200_set_owned_cells(self.h, p, mem))
+
+    def p2m(self, P: int = 10, precision: int = FP64):
+        self.P = P
+        self._check(self._L.tapas_b200_p2m(self.h, P, precision))
+
+    def m2m(self):
+        self._check(self._L.tapas_b200_m2m(self.h))
+
+    def multipoles(self, out=None):
+        """M as (ncells, NT) complex (host) or into `out`, a float64 buffer of
+        2 * ncells * NT values (host array or device tensor)."""
+        C = self.tree_info()["n_cells"]
+        nt = self.P * (self.P + 1) // 2
+        ret = out is None
+        if out is None:
+            out = np.zeros((C, nt, 2))
+        p, mem = _ptr(out)
+        self._check(self._L.tapas_b200_get_multipoles(self.h, p, mem))
+        return out[..., 0] + 1j * out[..., 1] if ret else out
+
+    def set_multipoles(self, M):
+        """M: a float64 buffer of 2 * ncells * NT values (host array or device tensor)."""
+        if isinstance(M, np.ndarray):
+            M = np.ascontiguousarray(M, dtype=np.float64)
+        p, mem = _ptr(M)
+        self._check(self._L.tapas_b200_set_multipoles(self.h, p, mem))
 
     def build_lists(self, theta: float = 0.4, mutual: int = 0):
         self._check(self._L.tapas_b200_build_lists(self.h, float(theta), mutual))

@@ -79,6 +79,18 @@ __global__ void __launch_bounds__(256) direct_kernel(const double *__restrict__ 
   }
 }
 
+// The non-empty leaves whose ownership mask has bit 1 (their bodies are
+// evaluated here); order is irrelevant (every leaf is independent).
+__global__ void select_owned_leaves(const int32_t *__restrict__ leaves, int64_t nl,
+                                    const uint8_t *__restrict__ own, int32_t *__restrict__ out,
+                                    int *__restrict__ count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nl;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = leaves[i];
+    if (own[c] & 2) out[atomicAdd(count, 1)] = c;
+  }
+}
+
 int copy_in(tapas_b200_ctx *ctx, double *dst, const double *src, int64_t n, int mem) {
   TB_CUDA(ctx, cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)n,
                                mem == TAPAS_B200_DEVICE ? cudaMemcpyDeviceToDevice
@@ -205,6 +217,11 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->bh_attr.release();
   ctx->bh_attr32.release();
   ctx->pinned.release();
+  for (int k = 0; k < kGemmSlabs; k++) {
+    if (ctx->gemm_streams[k]) cudaStreamDestroy(ctx->gemm_streams[k]);
+    if (ctx->gemm_join[k]) cudaEventDestroy(ctx->gemm_join[k]);
+  }
+  if (ctx->gemm_fork) cudaEventDestroy(ctx->gemm_fork);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return TAPAS_B200_OK;
@@ -266,6 +283,7 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
     return TAPAS_B200_ERR_ARG;
   }
   cudaStream_t s = ctx->stream;
+  ctx->timings = tapas_b200_timings{};  // a partition starts a new step's timings
   {
     PhaseTimer t(ctx, &ctx->timings.upload);
     TB_CUDA(ctx, ctx->x.ensure(n, s));
@@ -279,7 +297,45 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
   }
   ctx->n = n;
   ctx->have_bh_attr = false;
+  ctx->sharded = false;  // an ownership mask belongs to one tree
   return build_tree(ctx, ncrit);
+}
+
+int tapas_b200_set_owned_cells(tapas_b200_ctx *ctx, const uint8_t *mask, int mem) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_mem(ctx, mem));
+  if (!ctx->have_tree) {
+    set_error(ctx, "set_owned_cells: no tree (call partition first)");
+    return TAPAS_B200_ERR_STATE;
+  }
+  ctx->have_M = ctx->have_L = ctx->have_lists = false;
+  if (!mask) {
+    ctx->sharded = false;
+    return TAPAS_B200_OK;
+  }
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells, nl = ctx->n_nonempty_leaves;
+  TB_CUDA(ctx, ctx->cell_own.ensure(C + 1, s));
+  TB_CUDA(ctx, cudaMemcpyAsync(ctx->cell_own.p, mask, (size_t)C,
+                               mem == TAPAS_B200_DEVICE ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyHostToDevice,
+                               s));
+  TB_CUDA(ctx, ctx->leaf_own.ensure(nl + 1, s));
+  TB_CUDA(ctx, ctx->counters.ensure(8, s));
+  int *cnt = reinterpret_cast<int *>(ctx->counters.p);
+  TB_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(int), s));
+  if (nl > 0) {
+    select_owned_leaves<<<grid_for(nl, 256), 256, 0, s>>>(ctx->leaf_list.p, nl, ctx->cell_own.p,
+                                                           ctx->leaf_own.p, cnt);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  TB_CUDA(ctx, ctx->pinned.ensure(256));
+  int *h = reinterpret_cast<int *>(ctx->pinned.p);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->n_owned_leaves = h[0];
+  ctx->sharded = true;
+  return TAPAS_B200_OK;
 }
 
 int tapas_b200_bh_upward(tapas_b200_ctx *ctx) {
@@ -400,9 +456,73 @@ int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision) {
   ctx->have_M = ctx->have_L = false;
   ctx->P = P;
   ctx->precision = precision;
+  ctx->have_leaf_M = false;
   if (precision == TAPAS_B200_MIXED) TB_TRY(upward_fp32_p2m(ctx, P));
   else TB_TRY(upward_fp64(ctx, P));
   ctx->have_M = true;
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_p2m(tapas_b200_ctx *ctx, int P, int precision) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_precision(ctx, precision));
+  if (!ctx->have_tree) {
+    set_error(ctx, "p2m: no tree (call partition first)");
+    return TAPAS_B200_ERR_STATE;
+  }
+  if (P < kMinP || P > kMaxP) {
+    set_error(ctx, "p2m: expansion order P=%d outside %d..%d", P, kMinP, kMaxP);
+    return TAPAS_B200_ERR_UNSUPPORTED;
+  }
+  PhaseTimer t(ctx, &ctx->timings.upward);
+  ctx->have_M = ctx->have_L = false;
+  ctx->P = P;
+  ctx->precision = precision;
+  TB_TRY(p2m_only(ctx, P, precision == TAPAS_B200_MIXED));
+  ctx->have_leaf_M = true;
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_m2m(tapas_b200_ctx *ctx) {
+  TB_TRY(check_ctx(ctx));
+  if (!ctx->have_leaf_M) {
+    set_error(ctx, "m2m: needs p2m first");
+    return TAPAS_B200_ERR_STATE;
+  }
+  PhaseTimer t(ctx, &ctx->timings.m2m);
+  TB_TRY(m2m_only(ctx));
+  ctx->have_leaf_M = false;
+  ctx->have_M = true;
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_get_multipoles(tapas_b200_ctx *ctx, double *M, int mem) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_mem(ctx, mem));
+  if (!M || !(ctx->have_M || ctx->have_leaf_M)) {
+    set_error(ctx, "get_multipoles: null output or no multipoles");
+    return M ? TAPAS_B200_ERR_STATE : TAPAS_B200_ERR_ARG;
+  }
+  TB_CUDA(ctx, cudaMemcpyAsync(M, ctx->M.p, sizeof(double2) * (size_t)ctx->ncells * nterm_of(ctx->P),
+                               mem == TAPAS_B200_DEVICE ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  TB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_set_multipoles(tapas_b200_ctx *ctx, const double *M, int mem) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_mem(ctx, mem));
+  if (!M || !(ctx->have_M || ctx->have_leaf_M)) {
+    set_error(ctx, "set_multipoles: null input or no expansion order set (p2m first)");
+    return M ? TAPAS_B200_ERR_STATE : TAPAS_B200_ERR_ARG;
+  }
+  TB_CUDA(ctx, cudaMemcpyAsync(ctx->M.p, M, sizeof(double2) * (size_t)ctx->ncells * nterm_of(ctx->P),
+                               mem == TAPAS_B200_DEVICE ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyHostToDevice,
+                               ctx->stream));
+  TB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TAPAS_B200_OK;
 }
 

@@ -18,6 +18,7 @@ constexpr int kMaxDepth = 19;   // Morton<3, uint64_t>::MaxDepth(), sfc_morton.h
 constexpr int kDepthBits = 5;   // Morton<3, uint64_t>::DepthBits(), sfc_morton.h:154-163
 constexpr int kMinP = 2;
 constexpr int kMaxP = 16;
+constexpr int kGemmSlabs = 4;   // concurrent streams of the FP64 class GEMMs
 
 // ---------------------------------------------------------------------------
 // Error handling: every failure becomes a status code plus a message.
@@ -107,13 +108,20 @@ struct TcState {
   DBuf<uint32_t> pairs64;  // list indices of the pairs left to the FP64 kernel
   DBuf<int32_t> flag, scan, seg_start, tcflag, tcid, ntiles, tile_off;
   DBuf<int4> items;
+  DBuf<int2> cls_range;    // per selected class: first sorted pair, pair count
   DBuf<float> ops_hi, ops_lo, Mt, Lt;
+  DBuf<double> ops64, Mt64, Lt64;  // FP64 class GEMM (plain form)
+  DBuf<uint8_t> use64;     // FP64 class GEMM: list entries left to the pair kernel
+  DBuf<int32_t> oflag, opos;  // sharded: owned sorted pairs and their compacted positions
+  DBuf<uint8_t> sel, sel2;    // sharded: class selection per sorted / compacted pair
   DBuf<int> err;
   void release() {
     keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();
     pairs64.release(); flag.release(); scan.release(); seg_start.release(); tcflag.release();
-    tcid.release(); ntiles.release(); tile_off.release(); items.release(); ops_hi.release();
-    ops_lo.release(); Mt.release(); Lt.release(); err.release();
+    tcid.release(); ntiles.release(); tile_off.release(); items.release(); cls_range.release();
+    ops_hi.release(); ops_lo.release(); Mt.release(); Lt.release(); ops64.release();
+    Mt64.release(); Lt64.release(); use64.release(); oflag.release(); opos.release();
+    sel.release(); sel2.release(); err.release();
   }
 };
 
@@ -161,6 +169,13 @@ struct tapas_b200_ctx {
   tb::DBuf<int32_t> flag, flag_scan;    // per-level scratch
   tb::DBuf<int32_t> leaf_list;          // indices of non-empty leaves
   int64_t n_nonempty_leaves = 0;
+  // Sharded evaluation (tapas_b200_set_owned_cells): per cell bit 0 = this
+  // context computes the cell's local expansion, bit 1 = its bodies (P2M,
+  // P2P, L2P); cleared by each partition.
+  bool sharded = false;
+  tb::DBuf<uint8_t> cell_own;
+  tb::DBuf<int32_t> leaf_own;           // owned non-empty leaves
+  int64_t n_owned_leaves = 0;
 
   // ---- traversal lists ----
   bool have_lists = false;
@@ -204,6 +219,7 @@ struct tapas_b200_ctx {
   size_t tc_op_budget = (size_t)4 << 30;  // bytes of split-TF32 operators kept at once
   long long tc_wait_limit = 4000000000LL; // clock cycles a tensor-core M2L wait may take
   bool have_M = false, have_L = false;
+  bool have_leaf_M = false;             // p2m done, m2m not yet (M holds the leaves' only)
   tb::DBuf<double2> M, L;               // ncells x nterm complex FP64
   tb::DBuf<double> op_m2m, op_l2l;      // per level: child<->parent translation operators
   int level_ops_P = 0;                  // order the operators were built for (0: none)
@@ -218,6 +234,10 @@ struct tapas_b200_ctx {
   uint64_t bh_napprox = 0, bh_ndirect = 0;
 
   tb::HBuf pinned;
+  // FP64 class GEMMs: helper streams (and their fork / join events), made on first use
+  cudaStream_t gemm_streams[tb::kGemmSlabs] = {};
+  cudaEvent_t gemm_join[tb::kGemmSlabs] = {};
+  cudaEvent_t gemm_fork = nullptr;
 };
 
 namespace tb {
@@ -227,6 +247,17 @@ void mlp_release(tapas_b200_ctx *ctx);
 namespace tb {
 
 inline int nterm_of(int P) { return P * (P + 1) / 2; }
+
+// The non-empty leaves whose bodies this context evaluates: all of them, or
+// the owned ones of a sharded evaluation.
+inline const int32_t *work_leaves(const tapas_b200_ctx *ctx, int64_t &nl) {
+  nl = ctx->sharded ? ctx->n_owned_leaves : ctx->n_nonempty_leaves;
+  return ctx->sharded ? ctx->leaf_own.p : ctx->leaf_list.p;
+}
+// Per-cell ownership mask (bit 0: local expansion), or null when not sharded.
+inline const uint8_t *owned_cells(const tapas_b200_ctx *ctx) {
+  return ctx->sharded ? ctx->cell_own.p : nullptr;
+}
 
 inline void count_launch(tapas_b200_ctx *ctx) { ctx->launches++; }
 

@@ -17,6 +17,7 @@
 // leaf width).
 #include "expansions.cuh"
 #include "kernels.cuh"
+#include "m2l_tc.cuh"
 
 namespace tb {
 namespace {
@@ -166,8 +167,10 @@ __device__ __forceinline__ float warp_reduce_scatter16f(float (&buf)[16], int la
 // times the sum), 8 complex terms at a time summed over the warp by one
 // FP32 reduce-scatter, the sums over body chunks and the output in FP64.  A
 // term's rounding is ~6e-8 of itself and the warp's tree sum adds ~5 such
-// roundings, so M keeps ~1e-7 relative accuracy also when zero-mean charges
-// cancel.
+// roundings, so M's error stays near 1e-7 of the cell's multipoles of |q|
+// (measured below 1e-6 of them per cell); where zero-mean charges cancel, that
+// is more than 1e-7 of M itself (up to ~2e-5 of it measured), which the final
+// potential does not feel (it sums the same terms the cancellation removed).
 template <int P>
 __global__ void __launch_bounds__(kThreads) p2m32_kernel(
     const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
@@ -299,7 +302,8 @@ template <int P>
 __global__ void __launch_bounds__(kThreads) m2l_kernel(
     int64_t ncells, const int32_t *__restrict__ off, const uint64_t *__restrict__ list,
     uint64_t src_mask, const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
-    const double2 *__restrict__ M, double2 *__restrict__ L, const uint8_t *__restrict__ use) {
+    const double2 *__restrict__ M, double2 *__restrict__ L, const uint8_t *__restrict__ use,
+    const uint8_t *__restrict__ own) {
   using S = Sizes<P>;
   __shared__ cd Ysm[kWarps][S::NY];
   __shared__ cd Msm[kWarps][S::NT];
@@ -308,6 +312,7 @@ __global__ void __launch_bounds__(kThreads) m2l_kernel(
   if (c >= ncells) return;
   const int e0 = off[c], e1 = off[c + 1];
   if (e1 == e0 || cnb[c] == 0) return;
+  if (own && !(own[c] & 1)) return;  // sharded: another context's target
   cd *Y = Ysm[wi];
   cd *Mj = Msm[wi];
   cd acc[S::R];
@@ -866,6 +871,250 @@ __global__ void sum_octant_parts(const double *__restrict__ part, int64_t ncols,
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 M2L batched by offset class (plain form).  With M_n scaled by w^-n and
+// L_j by w^(j+1) (w = cell width), the M2L of every pair of one offset class
+// (level difference and centre offset in half-widths, m2l_tc.cu) is the same
+// real K x K map (K = 2 NT), so a class is one FP64 GEMM:
+//     Lt[:, targets] += T_class * Mt[:, sources].
+// A target has at most one source per class, and the classes run one launch
+// each in key order, so every target's sum has a fixed order (the FP64 form
+// stays bit-reproducible) without atomics.
+// ---------------------------------------------------------------------------
+
+// One block per class: the map's entries from the unit-offset singular
+// harmonics (evalLocal, :102-135), in FP64, stored transposed (row k = the
+// map's column k, targets contiguous) like the level operators.  Entry
+// (target (j,k), source (n,m)) collects the reference loop's m and -m terms
+// (:229-262) times (w_s / w_t)^n = 2^(delta n).
+template <int P>
+__global__ void __launch_bounds__(256) build_operators64(const uint64_t *__restrict__ keys,
+                                                         double *__restrict__ ops) {
+  using S = Sizes<P>;
+  constexpr int K = 2 * S::NT;
+  __shared__ cd Y[S::NY];
+  __shared__ double scale[P];
+  __shared__ unsigned char deg[S::NT], ord[S::NT];
+  const uint64_t key = keys[blockIdx.x];
+  const int delta = (int)((key >> 42) & 63) - 32;
+  const double Dx = (double)((long long)(key & 16383) - 8192);
+  const double Dy = (double)((long long)((key >> 14) & 16383) - 8192);
+  const double Dz = (double)((long long)((key >> 28) & 16383) - 8192);
+  const double u = ldexp(1.0, min(delta, 0) - 1);  // half-widths -> target widths
+  const Sph sp = sph_of(Dx * u, Dy * u, Dz * u);
+  if (threadIdx.x < P) {
+    local_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
+    scale[threadIdx.x] = ldexp(1.0, delta * (int)threadIdx.x);
+  }
+  for (int t = threadIdx.x; t < S::NT; t += blockDim.x) {
+    int j, k;
+    jk_of(t, j, k);
+    deg[t] = (unsigned char)j;
+    ord[t] = (unsigned char)k;
+  }
+  __syncthreads();
+  double *At = ops + (size_t)blockIdx.x * K * K;
+  for (int idx = threadIdx.x; idx < S::NT * S::NT; idx += blockDim.x) {
+    const int ti = idx / S::NT, to = idx - ti * S::NT;  // consecutive threads: targets
+    double v00 = 0, v01 = 0, v10 = 0, v11 = 0;  // [out re/im][in re/im]
+    const int j = deg[to], k = ord[to], n = deg[ti], ma = ord[ti];
+    if (n < P - j) {
+      const double Cnm = oddeven(j);
+      const int base = (j + n) * (j + n) + j + n - k;
+      const double C2 = Cnm * oddeven((k - ma) * (k < ma) + ma);
+      const cd Yp = Y[base + ma];
+      v00 = C2 * Yp.x;
+      v01 = -C2 * Yp.y;
+      v10 = C2 * Yp.y;
+      v11 = C2 * Yp.x;
+      if (ma > 0) {
+        const cd Ym = Y[base - ma];
+        v00 += Cnm * Ym.x;
+        v01 += Cnm * Ym.y;
+        v10 += Cnm * Ym.y;
+        v11 += -Cnm * Ym.x;
+      }
+      const double sc = scale[n];
+      v00 *= sc; v01 *= sc; v10 *= sc; v11 *= sc;
+    }
+    double *c_re = At + (size_t)(2 * ti) * K + 2 * to;
+    *reinterpret_cast<double2 *>(c_re) = make_double2(v00, v10);
+    *reinterpret_cast<double2 *>(c_re + K) = make_double2(v01, v11);
+  }
+}
+
+// Per cell (one warp each): Mt[c][2t + re/im] = M[c][t] / w^n, 0 for an empty cell.
+template <int P>
+__global__ void __launch_bounds__(256) normalize_M64(int64_t ncells, const int32_t *__restrict__ cnb,
+                                                     const double *__restrict__ cmin,
+                                                     const double *__restrict__ cmax,
+                                                     const double2 *__restrict__ M,
+                                                     double *__restrict__ Mt) {
+  using S = Sizes<P>;
+  constexpr int K = 2 * S::NT;
+  __shared__ double pw[kWarps][P];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int64_t nw = (int64_t)gridDim.x * kWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kWarps + wi; c < ncells; c += nw) {
+    const bool live = cnb[c] > 0;
+    __syncwarp();
+    if (live && lane < P) pw[wi][lane] = pow(cmax[3 * c] - cmin[3 * c], -lane);
+    __syncwarp();
+    for (int kk = lane; kk < K; kk += 32) {
+      double v = 0;
+      if (live) {
+        const double2 z = M[c * S::NT + (kk >> 1)];
+        v = ((kk & 1) ? z.y : z.x) * pw[wi][degree_of(kk >> 1)];
+      }
+      Mt[c * K + kk] = v;
+    }
+  }
+}
+
+// Per cell (one warp each): L[c][t] += (sum over the slabs, in slab order,
+// of Lt[c][2t, 2t+1]) / w^(j+1).
+template <int P>
+__global__ void __launch_bounds__(256) add_scaled_L64(int64_t ncells, const int32_t *__restrict__ cnb,
+                                                      const double *__restrict__ cmin,
+                                                      const double *__restrict__ cmax,
+                                                      const double *__restrict__ Lt,
+                                                      size_t slab, double2 *__restrict__ L) {
+  using S = Sizes<P>;
+  constexpr int K = 2 * S::NT;
+  __shared__ double pw[kWarps][P + 1];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int64_t nw = (int64_t)gridDim.x * kWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kWarps + wi; c < ncells; c += nw) {
+    if (cnb[c] == 0) continue;  // warp-uniform
+    __syncwarp();
+    if (lane <= P) pw[wi][lane] = pow(cmax[3 * c] - cmin[3 * c], -lane);
+    __syncwarp();
+    for (int t = lane; t < S::NT; t += 32) {
+      const double sc = pw[wi][degree_of(t) + 1];
+      double2 lt = *reinterpret_cast<const double2 *>(Lt + c * K + 2 * t);
+#pragma unroll
+      for (int k = 1; k < kGemmSlabs; k++) {
+        const double2 v = *reinterpret_cast<const double2 *>(Lt + k * slab + c * K + 2 * t);
+        lt.x += v.x;
+        lt.y += v.y;
+      }
+      const double2 o = L[c * S::NT + t];
+      L[c * S::NT + t] = make_double2(o.x + lt.x * sc, o.y + lt.y * sc);
+    }
+  }
+}
+
+// Streams the class GEMMs are spread over (and slabs of partial locals).
+int ensure_gemm_streams(tapas_b200_ctx *ctx) {
+  if (ctx->gemm_fork) return TAPAS_B200_OK;
+  for (int k = 0; k < kGemmSlabs; k++) {
+    TB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->gemm_streams[k], cudaStreamNonBlocking));
+    TB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->gemm_join[k], cudaEventDisableTiming));
+  }
+  TB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->gemm_fork, cudaEventDisableTiming));
+  return TAPAS_B200_OK;
+}
+
+// One class's GEMM: column p of the tile is pair vals[start + p] (source
+// multipole row in, target local row updated).  Tiling as level_gemm; a row
+// tile whose lowest degree is jmin reads only sources of degree < P - jmin.
+struct ClassGemm64 {
+  const double *At;      // K x K, row k = the map's column k
+  const uint32_t *vals;  // this class's pairs (list indices)
+  int len;
+  int shift;
+  const uint64_t *list;
+  const double *Mt;
+  double *Lt;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kGThreads, 3) class_gemm64(ClassGemm64 g) {
+  constexpr int K = P * (P + 1);
+  __shared__ __align__(16) double As[2][kGK][kGM];
+  __shared__ __align__(16) double Bs[2][kGK][kGN];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int r0 = blockIdx.y * kGM;
+  const int p0 = blockIdx.x * kGN;
+  const int wr = 32 * (w & 1) + 2 * (lane & 7);
+  const int tc = 16 * (w >> 1) + 4 * (lane >> 3);
+  const int am = 2 * (tid & 31), ak = tid >> 5;
+  const bool arow_ok = r0 + am < K;
+  const int bn = tid & 63, bk = 4 * (tid >> 6);
+  const uint64_t smask = (1ull << g.shift) - 1;
+  const bool bcol_ok = p0 + bn < g.len;
+  const double *bcol = nullptr;
+  if (bcol_ok) bcol = g.Mt + (int64_t)(g.list[g.vals[p0 + bn]] & smask) * K;
+  const int jmin = degree_of(r0 / 2);
+  const int kmax = min(K, (P - jmin) * (P - jmin + 1));
+  const int nchunks = (kmax + kGK - 1) / kGK;
+  double2 av[2], bv[2];
+  auto load_chunk = [&](int c) {
+    const int kc = c * kGK;
+#pragma unroll
+    for (int x = 0; x < 2; x++) {
+      const int kk = kc + ak + 8 * x;
+      av[x] = (kk < kmax && arow_ok)
+                  ? *reinterpret_cast<const double2 *>(g.At + (size_t)kk * K + r0 + am)
+                  : make_double2(0, 0);
+      const int kb = kc + bk + 2 * x;  // even; kmax is even
+      bv[x] = (kb < kmax && bcol_ok) ? *reinterpret_cast<const double2 *>(bcol + kb)
+                                     : make_double2(0, 0);
+    }
+  };
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0;
+  if (nchunks > 0) load_chunk(0);
+  for (int c = 0; c < nchunks; c++) {
+    const int buf = c & 1;
+#pragma unroll
+    for (int x = 0; x < 2; x++) {
+      *reinterpret_cast<double2 *>(&As[buf][ak + 8 * x][am]) = av[x];
+      Bs[buf][bk + 2 * x][bn] = bv[x].x;
+      Bs[buf][bk + 2 * x + 1][bn] = bv[x].y;
+    }
+    __syncthreads();
+    if (c + 1 < nchunks) load_chunk(c + 1);
+#pragma unroll
+    for (int k = 0; k < kGK; k++) {
+      const double2 a01 = *reinterpret_cast<const double2 *>(&As[buf][k][wr]);
+      const double2 a23 = *reinterpret_cast<const double2 *>(&As[buf][k][wr + 16]);
+      const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc]);
+      const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc + 2]);
+      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int p = p0 + tc + j;
+    if (p >= g.len) continue;
+    double *lcol = g.Lt + (int64_t)(g.list[g.vals[p]] >> g.shift) * K;
+#pragma unroll
+    for (int i = 0; i < 4; i += 2) {
+      const int row = r0 + wr + 8 * i;  // even; K is even
+      if (row >= K) continue;
+      double2 *dst = reinterpret_cast<double2 *>(lcol + row);
+      const double2 o = *dst;
+      *dst = make_double2(o.x + acc[i][j], o.y + acc[i + 1][j]);
+    }
+  }
+}
+
+__global__ void mark_list_entries(const uint32_t *__restrict__ idx, int64_t n,
+                                  uint8_t *__restrict__ use) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    use[idx[i]] = 1;
+}
+
 // Builds this tree's per-level operators for order P (levels 0 .. nlev-1 have
 // children).
 template <int P>
@@ -925,27 +1174,31 @@ int level_translate(tapas_b200_ctx *ctx, int l, const LevelFirstChild &lf, bool 
 }
 
 template <int P>
-int upward_P(tapas_b200_ctx *ctx, bool p2m_f32) {
+int p2m_P(tapas_b200_ctx *ctx, bool p2m_f32) {
   using S = Sizes<P>;
   cudaStream_t s = ctx->stream;
   const int64_t C = ctx->ncells;
   TB_CUDA(ctx, ctx->M.ensure((size_t)C * S::NT, s));
   TB_CUDA(ctx, cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
-  {
-    PhaseTimer t(ctx, &ctx->timings.p2m);
-    const int64_t nl = ctx->n_nonempty_leaves;
-    if (nl > 0 && p2m_f32) {
-      p2m32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-          ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
-          ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->M.p);
-      TB_LAUNCH_CHECK(ctx);
-    } else if (nl > 0) {
-      p2m_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-          ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
-          ctx->sz.p, ctx->sq.p, ctx->M.p);
-      TB_LAUNCH_CHECK(ctx);
-    }
+  PhaseTimer t(ctx, &ctx->timings.p2m);
+  int64_t nl = 0;
+  const int32_t *leaves = work_leaves(ctx, nl);  // sharded: owned leaves only
+  if (nl > 0 && p2m_f32) {
+    p2m32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p, ctx->sx.p,
+        ctx->sy.p, ctx->sz.p, ctx->sq.p, ctx->M.p);
+    TB_LAUNCH_CHECK(ctx);
+  } else if (nl > 0) {
+    p2m_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p, ctx->sz.p,
+        ctx->sq.p, ctx->M.p);
+    TB_LAUNCH_CHECK(ctx);
   }
+  return TAPAS_B200_OK;
+}
+
+template <int P>
+int m2m_P(tapas_b200_ctx *ctx) {
   PhaseTimer t(ctx, &ctx->timings.m2m);
   int nlev = 0;
   LevelFirstChild lf;
@@ -953,6 +1206,12 @@ int upward_P(tapas_b200_ctx *ctx, bool p2m_f32) {
   ctx->level_ops_P = P;
   for (int lev = nlev - 1; lev >= 0; lev--) TB_TRY(level_translate<P>(ctx, lev, lf, true));
   return TAPAS_B200_OK;
+}
+
+template <int P>
+int upward_P(tapas_b200_ctx *ctx, bool p2m_f32) {
+  TB_TRY(p2m_P<P>(ctx, p2m_f32));
+  return m2m_P<P>(ctx);
 }
 
 template <int P>
@@ -966,9 +1225,101 @@ int m2l_P(tapas_b200_ctx *ctx) {
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   m2l_kernel<P><<<(unsigned)((C + kWarps - 1) / kWarps), kThreads, 0, s>>>(
       C, ctx->m2l_off.p, ctx->m2l.p, mask, ctx->cnb.p, ctx->ccen.p, ctx->M.p, ctx->L.p,
-      nullptr);
+      nullptr, owned_cells(ctx));
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
+}
+
+// The plain form's M2L: classes of >= 32 pairs as FP64 GEMMs, the others by
+// the warp-per-target kernel over a pair mask (it writes L[target] first).
+template <int P>
+int m2l_gemm64_P(tapas_b200_ctx *ctx) {
+  using S = Sizes<P>;
+  constexpr int K = 2 * S::NT;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  const int64_t n = ctx->n_m2l;
+  auto &T = ctx->tc;
+  TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
+  TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
+  if (n == 0) return TAPAS_B200_OK;
+  M2LClassInfo ci;
+  {
+    PhaseTimer t(ctx, &ctx->timings.m2l_setup);
+    TB_TRY(m2l_classes(ctx, sizeof(double) * (size_t)K * K, ci));
+    if (ci.ntc > 0) {
+      TB_CUDA(ctx, T.ops64.ensure((size_t)K * K * ci.ntc, s));
+      build_operators64<P><<<(unsigned)ci.ntc, 256, 0, s>>>(T.tc_keys.p, T.ops64.p);
+      TB_LAUNCH_CHECK(ctx);
+      TB_CUDA(ctx, T.Mt64.ensure((size_t)C * K, s));
+      TB_CUDA(ctx, T.Lt64.ensure((size_t)kGemmSlabs * C * K, s));
+      normalize_M64<P><<<grid_for(C, kWarps, ctx->num_sms * 8), kThreads, 0, s>>>(
+          C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt64.p);
+      TB_LAUNCH_CHECK(ctx);
+      TB_CUDA(ctx, cudaMemsetAsync(T.Lt64.p, 0, sizeof(double) * kGemmSlabs * (size_t)C * K, s));
+    }
+  }
+  PhaseTimer t(ctx, &ctx->timings.m2l_fp64);
+  if (ci.n64 > 0) {
+    TB_CUDA(ctx, T.use64.ensure(n + 1, s));
+    TB_CUDA(ctx, cudaMemsetAsync(T.use64.p, 0, (size_t)n, s));
+    mark_list_entries<<<grid_for(ci.n64, 256), 256, 0, s>>>(T.pairs64.p, ci.n64, T.use64.p);
+    TB_LAUNCH_CHECK(ctx);
+    const uint64_t mask = (1ull << ctx->list_shift) - 1;
+    m2l_kernel<P><<<(unsigned)((C + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+        C, ctx->m2l_off.p, ctx->m2l.p, mask, ctx->cnb.p, ctx->ccen.p, ctx->M.p, ctx->L.p,
+        T.use64.p, nullptr);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  if (ci.ntc > 0) {
+    std::vector<int2> rng((size_t)ci.ntc);
+    std::vector<uint64_t> keys((size_t)ci.ntc);
+    TB_CUDA(ctx, cudaMemcpyAsync(rng.data(), T.cls_range.p, sizeof(int2) * ci.ntc,
+                                 cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaMemcpyAsync(keys.data(), T.tc_keys.p, sizeof(uint64_t) * ci.ntc,
+                                 cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaStreamSynchronize(s));
+    // A class runs on the helper stream of its slab and adds into that slab;
+    // the slab is a hash of the class key (not of its position in this list,
+    // which a sharded evaluation changes), a slab's classes run in key order
+    // (a fixed order per target), the slabs concurrently, and the slabs are
+    // added in slab order.
+    TB_TRY(ensure_gemm_streams(ctx));
+    TB_CUDA(ctx, cudaEventRecord(ctx->gemm_fork, s));
+    for (int k = 0; k < kGemmSlabs; k++)
+      TB_CUDA(ctx, cudaStreamWaitEvent(ctx->gemm_streams[k], ctx->gemm_fork, 0));
+    ClassGemm64 g;
+    g.list = ctx->m2l.p;
+    g.shift = ctx->list_shift;
+    g.Mt = T.Mt64.p;
+    for (int64_t c = 0; c < ci.ntc; c++) {  // key order
+      uint64_t hsh = keys[c] * 0x9E3779B97F4A7C15ull;
+      const int k = (int)((hsh ^ (hsh >> 29)) % kGemmSlabs);
+      g.Lt = T.Lt64.p + (size_t)k * C * K;
+      g.At = T.ops64.p + (size_t)c * K * K;
+      g.vals = T.vals.p + rng[c].x;
+      g.len = rng[c].y;
+      const dim3 grid((unsigned)((g.len + kGN - 1) / kGN), (unsigned)((K + kGM - 1) / kGM));
+      class_gemm64<P><<<grid, kGThreads, 0, ctx->gemm_streams[k]>>>(g);
+      TB_LAUNCH_CHECK(ctx);
+    }
+    for (int k = 0; k < kGemmSlabs; k++) {
+      TB_CUDA(ctx, cudaEventRecord(ctx->gemm_join[k], ctx->gemm_streams[k]));
+      TB_CUDA(ctx, cudaStreamWaitEvent(s, ctx->gemm_join[k], 0));
+    }
+    add_scaled_L64<P><<<grid_for(C, kWarps, ctx->num_sms * 8), kThreads, 0, s>>>(
+        C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, T.Lt64.p, (size_t)C * K, ctx->L.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  ctx->tc_classes = ci.ntc;
+  return TAPAS_B200_OK;
+}
+
+// P < 4: every pair by the warp-per-target kernel.
+template <int P>
+int m2l_fp64_P(tapas_b200_ctx *ctx) {
+  if constexpr (P < 4) return m2l_P<P>(ctx);
+  else return m2l_gemm64_P<P>(ctx);
 }
 
 template <int P>
@@ -1009,17 +1360,18 @@ int downward_P(tapas_b200_ctx *ctx, bool l2p_f32) {
     for (int lev = 0; lev < nlev; lev++) TB_TRY(level_translate<P>(ctx, lev, lf, false));
   }
   PhaseTimer t(ctx, &ctx->timings.l2p);
-  const int64_t nl = ctx->n_nonempty_leaves;
+  int64_t nl = 0;
+  const int32_t *leaves = work_leaves(ctx, nl);  // sharded: owned leaves only
   if (nl > 0 && l2p_f32) {
     l2p32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
+        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
         ctx->sx.p, ctx->sy.p,
         ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p,
         ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
     TB_LAUNCH_CHECK(ctx);
   } else if (nl > 0) {
     l2p_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
+        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->sx.p, ctx->sy.p,
         ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p, ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
     TB_LAUNCH_CHECK(ctx);
   }
@@ -1046,7 +1398,16 @@ template <int P>
 int upward_f32leaf_P(tapas_b200_ctx *ctx) { return upward_P<P>(ctx, true); }
 int upward_fp64(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_fp64_P) }
 int upward_fp32_p2m(tapas_b200_ctx *ctx, int P) { TB_DISPATCH_P(P, upward_f32leaf_P) }
-int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_P) }
+template <int P>
+int p2m_fp64_P(tapas_b200_ctx *ctx) { return p2m_P<P>(ctx, false); }
+template <int P>
+int p2m_f32leaf_P(tapas_b200_ctx *ctx) { return p2m_P<P>(ctx, true); }
+int p2m_only(tapas_b200_ctx *ctx, int P, bool fp32) {
+  if (fp32) { TB_DISPATCH_P(P, p2m_f32leaf_P) }
+  TB_DISPATCH_P(P, p2m_fp64_P)
+}
+int m2m_only(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2m_P) }
+int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_fp64_P) }
 
 static int m2l_pairs_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_pairs_P) }
 

@@ -7,6 +7,11 @@ namespace tb {
 int upward_fp64(tapas_b200_ctx *ctx, int P);
 // P2M in FP32 (FP64 sums and output), then FP64 M2M.
 int upward_fp32_p2m(tapas_b200_ctx *ctx, int P);
+// The two halves of the upward pass: P2M of the leaves this context
+// evaluates (M zeroed first; fp32: the mixed form's P2M), and the FP64 M2M of
+// the whole tree from the leaves' M (order ctx->P).
+int p2m_only(tapas_b200_ctx *ctx, int P, bool fp32);
+int m2m_only(tapas_b200_ctx *ctx);
 int m2l_fp64(tapas_b200_ctx *ctx);
 // L zeroed, then the FP64 M2L of the pairs at list indices pairs[0..npairs)
 // added into it (atomics: the order of a target's sums is not fixed).

@@ -243,6 +243,52 @@ __global__ void mark_fp64_pairs(const int32_t *__restrict__ scan, const int32_t 
   }
 }
 
+// Sharded evaluation: the sorted pairs whose target this context computes
+// (ownership bit 0), each with the selection its class got over ALL pairs,
+// so a pair takes the same path (GEMM or FP64 pair kernel) as in one context.
+__global__ void owned_pair_flags(const uint32_t *__restrict__ vals, int64_t n,
+                                 const uint64_t *__restrict__ list, int shift,
+                                 const uint8_t *__restrict__ own, const int32_t *__restrict__ scan,
+                                 const int32_t *__restrict__ flag,
+                                 const int32_t *__restrict__ tcflag, int32_t *__restrict__ oflag,
+                                 uint8_t *__restrict__ sel) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    oflag[i] = own[(int64_t)(list[vals[i]] >> shift)] & 1;
+    sel[i] = (uint8_t)tcflag[scan[i] + flag[i] - 1];
+  }
+}
+
+// Stable compaction of the owned sorted pairs (pos = exclusive scan of oflag).
+__global__ void compact_owned_pairs(const int32_t *__restrict__ oflag,
+                                    const int32_t *__restrict__ pos, int64_t n,
+                                    const uint64_t *__restrict__ keys,
+                                    const uint32_t *__restrict__ vals,
+                                    const uint8_t *__restrict__ sel, uint64_t *__restrict__ keys2,
+                                    uint32_t *__restrict__ vals2, uint8_t *__restrict__ sel2) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (!oflag[i]) continue;
+    const int32_t p = pos[i];
+    keys2[p] = keys[i];
+    vals2[p] = vals[i];
+    sel2[p] = sel[i];
+  }
+}
+
+// Per class of the compacted pairs: its selection and tile count.
+__global__ void class_flags_from_sel(const int32_t *__restrict__ seg_start, int64_t nseg,
+                                     int64_t n, const uint8_t *__restrict__ sel,
+                                     int32_t *__restrict__ tcflag, int32_t *__restrict__ ntiles) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
+    const bool tc = sel[b] != 0;
+    tcflag[c] = tc ? 1 : 0;
+    ntiles[c] = tc ? (int32_t)((e - b + kNTile - 1) / kNTile) : 0;
+  }
+}
+
 struct TileItem {
   int32_t cls;    // tensor-core class index (operator slot)
   int32_t start;  // first sorted pair index
@@ -255,13 +301,14 @@ __global__ void build_tiles(const int32_t *__restrict__ seg_start, int64_t nseg,
                             const int32_t *__restrict__ tile_off,
                             const uint64_t *__restrict__ keys, KeyPack kp,
                             uint64_t *__restrict__ tc_keys, TileItem *__restrict__ items,
-                            int *__restrict__ tc_pairs) {
+                            int2 *__restrict__ cls_range, int *__restrict__ tc_pairs) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg;
        c += (int64_t)gridDim.x * blockDim.x) {
     if (!tcflag[c]) continue;
     const int64_t b = seg_start[c], e = (c + 1 < nseg) ? seg_start[c + 1] : n;
     const int id = tcid[c];
     tc_keys[id] = kp.wide(keys[b]);
+    cls_range[id] = make_int2((int)b, (int)(e - b));
     atomicAdd(tc_pairs, (int)(e - b));
     int64_t o = tile_off[c];
     for (int64_t p = b; p < e; p += kNTile, o++) {
@@ -858,15 +905,19 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
   }
 }
 
-template <int P>
-int m2l_tc_P(tapas_b200_ctx *ctx) {
-  using S = TcShape<P>;
+}  // namespace
+
+// Offset classes of the current M2L list (steps 1-2 and the class/tile
+// tables of the header comment), for a GEMM whose operators take op_bytes per
+// class: ctx->tc holds the pairs sorted by class (vals), the selected
+// classes' wide keys (tc_keys), (first sorted pair, pair count) (cls_range)
+// and 128-pair tiles (items), and the list indices of the pairs left to the
+// FP64 pair path (pairs64).
+int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, M2LClassInfo &info) {
   cudaStream_t s = ctx->stream;
-  const int64_t C = ctx->ncells;
-  const int64_t n = ctx->n_m2l;
+  info = M2LClassInfo{};
+  int64_t n = ctx->n_m2l;  // pairs to evaluate here (sharded: of owned targets)
   auto &T = ctx->tc;
-  std::optional<PhaseTimer> setup_timer;
-  setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
   // 1. classify + stable sort by class key
   TB_CUDA(ctx, T.keys.ensure(n + 1, s));
   TB_CUDA(ctx, T.keys_alt.ensure(n + 1, s));
@@ -917,7 +968,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_TRY(scan_exclusive(ctx, T.flag.p, T.scan.p, n, T.scan.p + n));
   TB_CUDA(ctx, cudaMemcpyAsync(h, T.scan.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TB_CUDA(ctx, cudaStreamSynchronize(s));
-  const int64_t nseg = h[0];
+  int64_t nseg = h[0];
   TB_CUDA(ctx, T.seg_start.ensure(nseg + 1, s));
   TB_CUDA(ctx, T.tcflag.ensure(nseg + 1, s));
   TB_CUDA(ctx, T.tcid.ensure(nseg + 1, s));
@@ -930,7 +981,6 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   // holds, only the most populated ones run on the tensor cores.
   int64_t min_count = kTcMin;
   {
-    const size_t op_bytes = 2 * sizeof(float) * (size_t)S::MP * S::KP;
     const int64_t max_classes = std::max<int64_t>(1, (int64_t)(ctx->tc_op_budget / op_bytes));
     if (nseg > max_classes) {
       std::vector<int32_t> st(nseg);
@@ -947,6 +997,46 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p, kp,
                                                       min_count, T.tcflag.p, T.ntiles.p);
   TB_LAUNCH_CHECK(ctx);
+  int64_t nseg_all = nseg;
+  if (ctx->sharded) {
+    // keep the pairs whose target this context computes, with their classes'
+    // selection; then the classes of what is left
+    TB_CUDA(ctx, T.oflag.ensure(n + 1, s));
+    TB_CUDA(ctx, T.opos.ensure(n + 1, s));
+    TB_CUDA(ctx, T.sel.ensure(n + 1, s));
+    TB_CUDA(ctx, T.sel2.ensure(n + 1, s));
+    owned_pair_flags<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+        T.vals.p, n, ctx->m2l.p, ctx->list_shift, ctx->cell_own.p, T.scan.p, T.flag.p,
+        T.tcflag.p, T.oflag.p, T.sel.p);
+    TB_LAUNCH_CHECK(ctx);
+    TB_TRY(scan_exclusive(ctx, T.oflag.p, T.opos.p, n, T.opos.p + n));
+    compact_owned_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+        T.oflag.p, T.opos.p, n, T.keys.p, T.vals.p, T.sel.p, T.keys_alt.p, T.vals_alt.p,
+        T.sel2.p);
+    TB_LAUNCH_CHECK(ctx);
+    TB_CUDA(ctx, cudaMemcpyAsync(h, T.opos.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaStreamSynchronize(s));
+    std::swap(T.keys.p, T.keys_alt.p); std::swap(T.keys.cap, T.keys_alt.cap);
+    std::swap(T.vals.p, T.vals_alt.p); std::swap(T.vals.cap, T.vals_alt.cap);
+    n = h[0];
+    if (n == 0) {
+      ctx->tc_classes = ctx->tc_tiles = 0;
+      ctx->tc_segments = nseg_all;
+      return TAPAS_B200_OK;
+    }
+    segment_flags<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.keys.p, n, T.flag.p);
+    TB_LAUNCH_CHECK(ctx);
+    TB_TRY(scan_exclusive(ctx, T.flag.p, T.scan.p, n, T.scan.p + n));
+    TB_CUDA(ctx, cudaMemcpyAsync(h, T.scan.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaStreamSynchronize(s));
+    nseg = h[0];
+    segment_starts<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(T.flag.p, T.scan.p, n,
+                                                                      T.seg_start.p);
+    TB_LAUNCH_CHECK(ctx);
+    class_flags_from_sel<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.sel2.p,
+                                                              T.tcflag.p, T.ntiles.p);
+    TB_LAUNCH_CHECK(ctx);
+  }
   TB_TRY(scan_exclusive(ctx, T.tcflag.p, T.tcid.p, nseg, T.tcid.p + nseg));
   TB_TRY(scan_exclusive(ctx, T.ntiles.p, T.tile_off.p, nseg, T.tile_off.p + nseg));
   TB_CUDA(ctx, cudaMemsetAsync(T.err.p + 3, 0, sizeof(int), s));
@@ -961,17 +1051,45 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   const int64_t ntc = h[0], nitems = h[1], n64 = h[2];
   ctx->tc_classes = ntc;
   ctx->tc_tiles = nitems;
-  ctx->tc_segments = nseg;
-  // 3. operators
+  ctx->tc_segments = nseg_all;
+  // 3. class tables
   TB_CUDA(ctx, T.tc_keys.ensure(ntc + 1, s));
+  TB_CUDA(ctx, T.cls_range.ensure(ntc + 1, s));
   TB_CUDA(ctx, T.items.ensure((size_t)(nitems + 1) * sizeof(TileItem) / 16 + 1, s));
   TB_CUDA(ctx, T.err.ensure(4, s));
   TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
   build_tiles<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.tcflag.p, T.tcid.p,
                                                    T.tile_off.p, T.keys.p, kp, T.tc_keys.p,
                                                    reinterpret_cast<TileItem *>(T.items.p),
-                                                   T.err.p + 1);
+                                                   T.cls_range.p, T.err.p + 1);
   TB_LAUNCH_CHECK(ctx);
+  info.nseg = nseg;
+  info.ntc = ntc;
+  info.nitems = nitems;
+  info.n64 = n64;
+  return TAPAS_B200_OK;
+}
+
+namespace {
+
+template <int P>
+int m2l_tc_P(tapas_b200_ctx *ctx) {
+  using S = TcShape<P>;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  const int64_t n = ctx->n_m2l;
+  auto &T = ctx->tc;
+  std::optional<PhaseTimer> setup_timer;
+  setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
+  M2LClassInfo ci;
+  TB_TRY(m2l_classes(ctx, 2 * sizeof(float) * (size_t)S::MP * S::KP, ci));
+  if (n == 0) {  // no M2L pair: every local expansion is zero
+    TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
+    TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
+    return TAPAS_B200_OK;
+  }
+  const int64_t ntc = ci.ntc, nitems = ci.nitems, n64 = ci.n64;
+  int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
   const size_t opsz = (size_t)S::MP * S::KP;
   if (ntc > 0) {
     TB_CUDA(ctx, T.ops_hi.ensure(opsz * ntc, s));

@@ -562,13 +562,14 @@ __global__ void __launch_bounds__(kMixedThreads, kBlocks) p2p_mixed_kernel(
 // queue order (ctx->p2p_order: items by decreasing work).
 int p2p_items(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
-  const int64_t nl = ctx->n_nonempty_leaves;
+  int64_t nl = 0;
+  const int32_t *leaves = work_leaves(ctx, nl);  // sharded: owned target leaves
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
   TB_CUDA(ctx, ctx->p2p_kcnt.ensure(nl + 1, s));
   TB_CUDA(ctx, ctx->p2p_koff.ensure(nl + 1, s));
   TB_CUDA(ctx, ctx->p2p_psz.ensure(nl + 1, s));
   TB_CUDA(ctx, ctx->p2p_poff.ensure(nl + 1, s));
-  leaf_pieces<<<grid_for(nl, 256), 256, 0, s>>>(ctx->leaf_list.p, nl, ctx->p2p_off.p, ctx->p2p.p,
+  leaf_pieces<<<grid_for(nl, 256), 256, 0, s>>>(leaves, nl, ctx->p2p_off.p, ctx->p2p.p,
                                                  mask, ctx->cnb.p, ctx->p2p_kcnt.p,
                                                  ctx->p2p_psz.p);
   TB_LAUNCH_CHECK(ctx);
@@ -595,7 +596,7 @@ int p2p_items(tapas_b200_ctx *ctx) {
   TB_CUDA(ctx, ctx->p2p_order_alt.ensure(ni + 1, s));
   TB_CUDA(ctx, ctx->p2p_counter.ensure(4, s));
   emit_items<<<grid_for(nl, 256), 256, 0, s>>>(
-      ctx->leaf_list.p, nl, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cnb.p, ctx->p2p_kcnt.p,
+      leaves, nl, ctx->p2p_off.p, ctx->p2p.p, mask, ctx->cnb.p, ctx->p2p_kcnt.p,
       ctx->p2p_koff.p, ctx->p2p_poff.p, reinterpret_cast<WorkItem *>(ctx->p2p_items.p),
       ctx->p2p_wkey.p, ctx->p2p_order.p, ctx->p2p_part.p);
   TB_LAUNCH_CHECK(ctx);
@@ -617,9 +618,10 @@ int p2p_items(tapas_b200_ctx *ctx) {
 // Adds the pieces of split leaves into trg (after a P2P kernel).
 int p2p_finish(tapas_b200_ctx *ctx) {
   if (!ctx->p2p_split) return TAPAS_B200_OK;
-  const int64_t nl = ctx->n_nonempty_leaves;
+  int64_t nl = 0;
+  const int32_t *leaves = work_leaves(ctx, nl);
   split_reduce<<<grid_for(nl, 256), 256, 0, ctx->stream>>>(
-      ctx->leaf_list.p, nl, ctx->cbeg.p, ctx->cnb.p, ctx->p2p_kcnt.p, ctx->p2p_poff.p,
+      leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->p2p_kcnt.p, ctx->p2p_poff.p,
       ctx->p2p_part.p, ctx->trg.p);
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
@@ -635,9 +637,19 @@ int p2p_grid(tapas_b200_ctx *ctx, int warps_per_block) {
 
 }  // namespace
 
+// Sharded: the rows of bodies another context evaluates are exactly zero, so
+// the contexts' results add up without changing a bit.
+static int zero_results_if_sharded(tapas_b200_ctx *ctx) {
+  if (ctx->sharded)
+    TB_CUDA(ctx, cudaMemsetAsync(ctx->trg.p, 0, sizeof(double) * 4 * (size_t)ctx->n, ctx->stream));
+  return TAPAS_B200_OK;
+}
+
 int p2p_fp64(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
-  const int64_t nl = ctx->n_nonempty_leaves;
+  TB_TRY(zero_results_if_sharded(ctx));
+  int64_t nl = 0;
+  work_leaves(ctx, nl);
   if (nl == 0) return TAPAS_B200_OK;
   TB_TRY(p2p_items(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
@@ -651,8 +663,11 @@ int p2p_fp64(tapas_b200_ctx *ctx) {
 
 int p2p_mixed(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
-  const int64_t nl = ctx->n_nonempty_leaves;
-  if (nl == 0) return TAPAS_B200_OK;
+  TB_TRY(zero_results_if_sharded(ctx));
+  int64_t nw = 0;
+  work_leaves(ctx, nw);
+  if (nw == 0) return TAPAS_B200_OK;
+  const int64_t nl = ctx->n_nonempty_leaves;  // every source leaf needs its offsets
   TB_CUDA(ctx, ctx->rel4.ensure(ctx->n, s));
   TB_CUDA(ctx, ctx->rel_lo.ensure(ctx->n, s));
   prepare_rel<<<(unsigned)((nl + 7) / 8), 256, 0, s>>>(ctx->leaf_list.p, nl, ctx->cbeg.p,
