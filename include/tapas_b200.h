@@ -225,6 +225,40 @@ int tapas_b200_p2p(tapas_b200_ctx *ctx, int precision);
  * (:275-307) for every non-empty leaf. */
 int tapas_b200_downward(tapas_b200_ctx *ctx, int precision);
 
+/* ---- device views for user functors -------------------------------------- */
+/* The reference offloads any __host__ __device__ body-pair functor through
+ * its vectormap (cpp/include/tapas/vectormap_cuda.h:645-1005).  The templates
+ * of include/tapas_b200/device.cuh do the same on this library's tree and
+ * lists, compiled into the user's program by nvcc; this view gives them the
+ * context's device arrays (read-only, valid until the next call that rebuilds
+ * the tree or the lists).  Cells are in get_cells order; bodies in Morton
+ * order; lists as build_lists left them (CSR by target cell, entries
+ * target << list_shift | source, NULL before the first build_lists). */
+#define TAPAS_B200_MAX_LEVELS 24
+typedef struct {
+  int64_t n_bodies, n_cells, n_levels;
+  int64_t level_off[TAPAS_B200_MAX_LEVELS + 1]; /* host values: cells of level l are
+                                                   [level_off[l], level_off[l+1]) */
+  const int32_t *nb, *bbeg, *leaf, *parent, *child0, *level;
+  const double *center3, *min3, *max3;          /* 3 values per cell */
+  const double *x, *y, *z, *q;                  /* bodies, Morton order */
+  const uint32_t *orig_index;                   /* Morton position -> caller's index */
+  const int32_t *p2p_off, *m2l_off;             /* n_cells + 1 each */
+  const uint64_t *p2p_list, *m2l_list;
+  int64_t n_p2p, n_m2l;
+  int32_t list_shift;
+} tapas_b200_device_view;
+int tapas_b200_get_device_view(tapas_b200_ctx *ctx, tapas_b200_device_view *out);
+/* The cudaStream_t the context issues its work on (for the caller's kernels). */
+int tapas_b200_get_stream(tapas_b200_ctx *ctx, void **stream);
+/* Near field computed by the caller's own P2P functor (in place of
+ * tapas_b200_p2p), 4 values per body in Morton order, in the reference's P2P
+ * convention (sums of q_i q_j / r and q_i q_j dX / r^3, which the FP64 L2P
+ * divides by q_i, ex/LaplaceSphericalCPU_tapas.h:283); host or device memory.
+ * tapas_b200_downward then adds the far field to it.  No counterpart call in
+ * the reference (its P2P writes the body attributes directly). */
+int tapas_b200_set_near_field(tapas_b200_ctx *ctx, const double *trg4, int mem);
+
 /* ---- sharded evaluation over several GPUs -------------------------------- */
 /* The reference splits the work over MPI ranks by Morton-key ranges and builds
  * a locally essential tree per rank (cpp/include/tapas/hot/buildtree.h:

@@ -43,6 +43,9 @@
 #include <vector>
 
 #include "../tapas_b200.h"
+#ifdef __CUDACC__
+#include "device.cuh"
+#endif
 
 namespace tapas {
 
@@ -216,6 +219,69 @@ class Cell {
     for (size_t i = 0; i < n; i++) b200::AttrStore<BodyAttr>::set(attrs_[i], &t[4 * i]);
   }
   void check_(int rc) const { b200::check(rc, ctx_); }
+#ifdef __CUDACC__
+  // The user's P2P functor over the context's leaf pairs, on device copies
+  // of the bodies (BodyAttr starts value-initialised); the near field goes
+  // back to the library for the L2P.  BodyAttr must be the four doubles of
+  // ExaFMM's kvec4 (pot, ax, ay, az).
+  template <class F>
+  void user_p2p_(F f) {
+    static_assert(sizeof(BodyAttr) == 4 * sizeof(double),
+                  "the near field is four doubles per body (ExaFMM kvec4)");
+    const size_t n = bodies_.size();
+    Body *db = nullptr;
+    BodyAttr *da = nullptr;
+    const std::vector<BodyAttr> zero(n, BodyAttr());
+    int rc = cudaMalloc(&db, sizeof(Body) * n) == cudaSuccess &&
+                     cudaMalloc(&da, sizeof(BodyAttr) * n) == cudaSuccess
+                 ? TAPAS_B200_OK
+                 : TAPAS_B200_ERR_NOMEM;
+    if (rc == TAPAS_B200_OK &&
+        (cudaMemcpy(db, bodies_.data(), sizeof(Body) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(da, zero.data(), sizeof(BodyAttr) * n, cudaMemcpyHostToDevice) != cudaSuccess))
+      rc = TAPAS_B200_ERR_CUDA;
+    if (rc == TAPAS_B200_OK) rc = b200::Map2LeafPairs(ctx_, db, da, f);
+    if (rc == TAPAS_B200_OK)
+      rc = tapas_b200_set_near_field(ctx_, reinterpret_cast<const double *>(da),
+                                     TAPAS_B200_DEVICE);
+    void *s = nullptr;
+    tapas_b200_get_stream(ctx_, &s);
+    if (cudaStreamSynchronize(static_cast<cudaStream_t>(s)) != cudaSuccess && rc == TAPAS_B200_OK)
+      rc = TAPAS_B200_ERR_CUDA;
+    cudaFree(db);
+    cudaFree(da);
+    if (rc != TAPAS_B200_OK && rc != TAPAS_B200_ERR_STATE)
+      throw b200::Error(rc, std::string("user P2P functor: ") + tapas_b200_last_error(ctx_));
+    check_(rc);
+  }
+  // MapReduce over the tree (device.cuh) with the root's bodies; values in
+  // get_cells order.
+  template <class T, class LeafF, class Op, class PostF>
+  std::vector<T> map_reduce_(LeafF leaf, Op op, PostF post) {
+    const size_t n = bodies_.size(), C = (size_t)info_.n_cells;
+    Body *db = nullptr;
+    T *dv = nullptr;
+    std::vector<T> out(C);
+    int rc = cudaMalloc(&db, sizeof(Body) * n) == cudaSuccess &&
+                     cudaMalloc(&dv, sizeof(T) * C) == cudaSuccess
+                 ? TAPAS_B200_OK
+                 : TAPAS_B200_ERR_NOMEM;
+    if (rc == TAPAS_B200_OK &&
+        cudaMemcpy(db, bodies_.data(), sizeof(Body) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = TAPAS_B200_ERR_CUDA;
+    if (rc == TAPAS_B200_OK) rc = b200::MapReduce(ctx_, db, dv, leaf, op, post);
+    void *s = nullptr;
+    tapas_b200_get_stream(ctx_, &s);
+    if (rc == TAPAS_B200_OK &&
+        (cudaStreamSynchronize(static_cast<cudaStream_t>(s)) != cudaSuccess ||
+         cudaMemcpy(out.data(), dv, sizeof(T) * C, cudaMemcpyDeviceToHost) != cudaSuccess))
+      rc = TAPAS_B200_ERR_CUDA;
+    cudaFree(db);
+    cudaFree(dv);
+    check_(rc);
+    return out;
+  }
+#endif
 
  private:
   tapas_b200_ctx *ctx_ = nullptr;
@@ -224,6 +290,19 @@ class Cell {
   std::vector<BodyAttr> attrs_;
   bool mutual_ = false;
 };
+
+#ifdef __CUDACC__
+// FMM_DTT with the user's own body-pair functor for the near field, the
+// reference's P2P offload through its vectormap (the traversal's leaf pairs
+// go to Map2LeafPairs; include/tapas_b200/device.cuh).  The functor is called
+// as p2p(Body &bi, BodyAttr &ai, Body &bj, BodyAttr &aj) on the device, one
+// thread per target body; a reference functor with the extra (Xperiodic,
+// mutual) arguments is wrapped by a functor that passes them.
+template <class P2PFunctor>
+struct FMM_DTT_With {
+  P2PFunctor p2p;
+};
+#endif
 
 template <class CELL>
 struct ProductIterator {
@@ -290,6 +369,30 @@ struct Tapas {
       prod.t1_.fetch_results_();
     }
   }
+
+#ifdef __CUDACC__
+  // FMM_DTT with the user's P2P functor (args: mutual, nspawn, theta): lists
+  // and M2L by the library, the near field by the functor on the device.
+  template <class F, class... Args>
+  static void Map(FMM_DTT_With<F> fn, ProductIterator<Cell> prod, Args... args) {
+    static_assert(sizeof...(args) == 3, "FMM_DTT takes (mutual, nspawn, theta)");
+    if (&prod.t1_ != &prod.t2_) throw b200::Error(TAPAS_B200_ERR_ARG, "Product(root, root) only");
+    const double a[] = {(double)args...};
+    Cell &c = prod.t1_;
+    c.check_(tapas_b200_build_lists(c.context(), a[2], (int)a[0]));
+    c.check_(tapas_b200_m2l(c.context(), b200::options().precision));
+    c.user_p2p_(fn.p2p);
+  }
+
+  // MapReduce (the reference's proposed Reduce API, bh_reduce.cc:186):
+  // per cell, children before parents, leaf(cell, bodies, nb) at leaves and
+  // op folded over the 8 children in order elsewhere, then post(cell, value);
+  // device functors; values in get_cells order.
+  template <class T, class LeafF, class Op, class PostF>
+  static std::vector<T> MapReduce(Cell &c, LeafF leaf, Op op, PostF post) {
+    return c.template map_reduce_<T>(leaf, op, post);
+  }
+#endif
 };
 
 }  // namespace tapas

@@ -1,4 +1,5 @@
 // C ABI of libtapas_b200 (declared in include/tapas_b200.h).
+#include <algorithm>
 #include <cstring>
 #include <new>
 
@@ -299,6 +300,75 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
   ctx->have_bh_attr = false;
   ctx->sharded = false;  // an ownership mask belongs to one tree
   return build_tree(ctx, ncrit);
+}
+
+int tapas_b200_get_device_view(tapas_b200_ctx *ctx, tapas_b200_device_view *out) {
+  TB_TRY(check_ctx(ctx));
+  if (!out) {
+    set_error(ctx, "get_device_view: null output");
+    return TAPAS_B200_ERR_ARG;
+  }
+  if (!ctx->have_tree) {
+    set_error(ctx, "get_device_view: no tree (call partition first)");
+    return TAPAS_B200_ERR_STATE;
+  }
+  *out = tapas_b200_device_view{};
+  out->n_bodies = ctx->n;
+  out->n_cells = ctx->ncells;
+  const int64_t nlev = std::min<int64_t>((int64_t)ctx->level_off.size() - 1,
+                                         TAPAS_B200_MAX_LEVELS);
+  out->n_levels = nlev;
+  for (int64_t l = 0; l <= nlev; l++) out->level_off[l] = ctx->level_off[(size_t)l];
+  out->nb = ctx->cnb.p;
+  out->bbeg = ctx->cbeg.p;
+  out->leaf = ctx->cleaf.p;
+  out->parent = ctx->cparent.p;
+  out->child0 = ctx->cchild.p;
+  out->level = ctx->clevel.p;
+  out->center3 = ctx->ccen.p;
+  out->min3 = ctx->cmin.p;
+  out->max3 = ctx->cmax.p;
+  out->x = ctx->sx.p;
+  out->y = ctx->sy.p;
+  out->z = ctx->sz.p;
+  out->q = ctx->sq.p;
+  out->orig_index = ctx->idx.p;
+  if (ctx->have_lists) {
+    out->p2p_off = ctx->p2p_off.p;
+    out->m2l_off = ctx->m2l_off.p;
+    out->p2p_list = ctx->p2p.p;
+    out->m2l_list = ctx->m2l.p;
+    out->n_p2p = ctx->n_p2p;
+    out->n_m2l = ctx->n_m2l;
+    out->list_shift = ctx->list_shift;
+  }
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_set_near_field(tapas_b200_ctx *ctx, const double *trg4, int mem) {
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_mem(ctx, mem));
+  if (!trg4) {
+    set_error(ctx, "set_near_field: null input");
+    return TAPAS_B200_ERR_ARG;
+  }
+  if (!ctx->have_tree) {
+    set_error(ctx, "set_near_field: no tree (call partition first)");
+    return TAPAS_B200_ERR_STATE;
+  }
+  TB_CUDA(ctx, cudaMemcpyAsync(ctx->trg.p, trg4, sizeof(double) * 4 * (size_t)ctx->n,
+                               mem == TAPAS_B200_DEVICE ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyHostToDevice,
+                               ctx->stream));
+  ctx->near_precision = TAPAS_B200_FP64;  // sums carry q_i: the L2P divides by it
+  return TAPAS_B200_OK;
+}
+
+int tapas_b200_get_stream(tapas_b200_ctx *ctx, void **stream) {
+  TB_TRY(check_ctx(ctx));
+  if (!stream) return TAPAS_B200_ERR_ARG;
+  *stream = ctx->stream;
+  return TAPAS_B200_OK;
 }
 
 int tapas_b200_set_owned_cells(tapas_b200_ctx *ctx, const uint8_t *mask, int mem) {
@@ -651,10 +721,19 @@ int tapas_b200_get_results(tapas_b200_ctx *ctx, double *trg4, int order, int mem
   const int64_t n = ctx->n;
   const double *src = ctx->trg.p;
   if (order == TAPAS_B200_ORDER_ORIGINAL) {
-    TB_CUDA(ctx, ctx->trg_out.ensure(4 * n, s));
+    // device output: scattered straight into the caller's buffer
+    double *dst = trg4;
+    if (mem == TAPAS_B200_HOST) {
+      TB_CUDA(ctx, ctx->trg_out.ensure(4 * n, s));
+      dst = ctx->trg_out.p;
+    }
     scatter_results<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(ctx->trg.p, ctx->idx.p, n,
-                                                                         ctx->trg_out.p);
+                                                                         dst);
     TB_LAUNCH_CHECK(ctx);
+    if (mem == TAPAS_B200_DEVICE) {
+      TB_CUDA(ctx, cudaStreamSynchronize(s));
+      return TAPAS_B200_OK;
+    }
     src = ctx->trg_out.p;
   }
   TB_CUDA(ctx, cudaMemcpyAsync(trg4, src, 32 * (size_t)n,

@@ -99,6 +99,9 @@ class TorchComm:
         self.dist = dist
         self.rank = dist.get_rank()
         self.size = dist.get_world_size()
+        if device is None and dist.get_backend() == "nccl":  # NCCL takes device tensors only
+            import torch
+            device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
 
     def _tensor(self, a):
@@ -127,8 +130,10 @@ class TorchComm:
         if isinstance(a, torch.Tensor):
             self.dist.all_reduce(a, op=self.dist.ReduceOp.SUM)
             return a
-        t = torch.from_numpy(a)
+        t = self._tensor(a)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        if t.device.type != "cpu":
+            a[...] = t.cpu().numpy()
         return a
 
 
