@@ -299,6 +299,7 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
   ctx->n = n;
   ctx->have_bh_attr = false;
   ctx->sharded = false;  // an ownership mask belongs to one tree
+  ctx->tc.mt_ready = false;
   return build_tree(ctx, ncrit);
 }
 
@@ -527,8 +528,14 @@ int tapas_b200_upward(tapas_b200_ctx *ctx, int P, int precision) {
   ctx->P = P;
   ctx->precision = precision;
   ctx->have_leaf_M = false;
-  if (precision == TAPAS_B200_MIXED) TB_TRY(upward_fp32_p2m(ctx, P));
-  else TB_TRY(upward_fp64(ctx, P));
+  ctx->tc.mt_ready = false;
+  if (precision == TAPAS_B200_MIXED) {
+    TB_TRY(p2m_only(ctx, P, true));
+    PhaseTimer tm(ctx, &ctx->timings.m2m);
+    TB_TRY(tc_tree_upward(ctx));
+  } else {
+    TB_TRY(upward_fp64(ctx, P));
+  }
   ctx->have_M = true;
   return TAPAS_B200_OK;
 }
@@ -548,6 +555,7 @@ int tapas_b200_p2m(tapas_b200_ctx *ctx, int P, int precision) {
   ctx->have_M = ctx->have_L = false;
   ctx->P = P;
   ctx->precision = precision;
+  ctx->tc.mt_ready = false;
   TB_TRY(p2m_only(ctx, P, precision == TAPAS_B200_MIXED));
   ctx->have_leaf_M = true;
   return TAPAS_B200_OK;
@@ -560,7 +568,8 @@ int tapas_b200_m2m(tapas_b200_ctx *ctx) {
     return TAPAS_B200_ERR_STATE;
   }
   PhaseTimer t(ctx, &ctx->timings.m2m);
-  TB_TRY(m2m_only(ctx));
+  if (ctx->precision == TAPAS_B200_MIXED) TB_TRY(tc_tree_upward(ctx));
+  else TB_TRY(m2m_only(ctx));
   ctx->have_leaf_M = false;
   ctx->have_M = true;
   return TAPAS_B200_OK;

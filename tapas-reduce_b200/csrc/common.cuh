@@ -114,6 +114,14 @@ struct TcState {
   DBuf<uint8_t> use64;     // FP64 class GEMM: list entries left to the pair kernel
   DBuf<int32_t> oflag, opos;  // sharded: owned sorted pairs and their compacted positions
   DBuf<uint8_t> sel, sel2;    // sharded: class selection per sorted / compacted pair
+  // tensor-core M2M of the mixed form
+  DBuf<float> ops_tr_hi, ops_tr_lo;  // 8 M2M classes: octant o
+  int tr_P = 0;                      // order they were built for (0: none)
+  DBuf<uint64_t> tree_list;          // one level's (parent << 32 | child) pairs
+  DBuf<uint32_t> iota;               // 0, 1, 2, ... (pair order of a level)
+  int64_t iota_n = 0;
+  DBuf<int4> tree_items;             // one level's 128-pair tiles
+  bool mt_ready = false;             // Mt holds this tree's normalised split multipoles
   DBuf<int> err;
   void release() {
     keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();
@@ -121,7 +129,11 @@ struct TcState {
     tcid.release(); ntiles.release(); tile_off.release(); items.release(); cls_range.release();
     ops_hi.release(); ops_lo.release(); Mt.release(); Lt.release(); ops64.release();
     Mt64.release(); Lt64.release(); use64.release(); oflag.release(); opos.release();
-    sel.release(); sel2.release(); err.release();
+    sel.release(); sel2.release(); ops_tr_hi.release(); ops_tr_lo.release(); tree_list.release();
+    iota.release(); tree_items.release(); err.release();
+    tr_P = 0;
+    iota_n = 0;
+    mt_ready = false;
   }
 };
 

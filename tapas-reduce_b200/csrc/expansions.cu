@@ -1208,6 +1208,18 @@ int m2m_P(tapas_b200_ctx *ctx) {
   return TAPAS_B200_OK;
 }
 
+// FP64 M2M level GEMMs of the parent levels max_levels - 1 .. 0 only.
+template <int P>
+int fp64_m2m_levels_P(tapas_b200_ctx *ctx, int max_levels) {
+  int nlev = 0;
+  LevelFirstChild lf;
+  TB_TRY(build_level_ops<P>(ctx, nlev, lf));  // the upward pass builds them for this tree
+  ctx->level_ops_P = P;
+  for (int lev = std::min(nlev, max_levels) - 1; lev >= 0; lev--)
+    TB_TRY(level_translate<P>(ctx, lev, lf, true));
+  return TAPAS_B200_OK;
+}
+
 template <int P>
 int upward_P(tapas_b200_ctx *ctx, bool p2m_f32) {
   TB_TRY(p2m_P<P>(ctx, p2m_f32));
@@ -1407,6 +1419,29 @@ int p2m_only(tapas_b200_ctx *ctx, int P, bool fp32) {
   TB_DISPATCH_P(P, p2m_fp64_P)
 }
 int m2m_only(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2m_P) }
+
+int fp64_m2m_levels(tapas_b200_ctx *ctx, int max_levels) {
+  switch (ctx->P) {
+    case 2: return fp64_m2m_levels_P<2>(ctx, max_levels);
+    case 3: return fp64_m2m_levels_P<3>(ctx, max_levels);
+    case 4: return fp64_m2m_levels_P<4>(ctx, max_levels);
+    case 5: return fp64_m2m_levels_P<5>(ctx, max_levels);
+    case 6: return fp64_m2m_levels_P<6>(ctx, max_levels);
+    case 7: return fp64_m2m_levels_P<7>(ctx, max_levels);
+    case 8: return fp64_m2m_levels_P<8>(ctx, max_levels);
+    case 9: return fp64_m2m_levels_P<9>(ctx, max_levels);
+    case 10: return fp64_m2m_levels_P<10>(ctx, max_levels);
+    case 11: return fp64_m2m_levels_P<11>(ctx, max_levels);
+    case 12: return fp64_m2m_levels_P<12>(ctx, max_levels);
+    case 13: return fp64_m2m_levels_P<13>(ctx, max_levels);
+    case 14: return fp64_m2m_levels_P<14>(ctx, max_levels);
+    case 15: return fp64_m2m_levels_P<15>(ctx, max_levels);
+    case 16: return fp64_m2m_levels_P<16>(ctx, max_levels);
+    default: break;
+  }
+  set_error(ctx, "expansion order P=%d outside %d..%d", ctx->P, kMinP, kMaxP);
+  return TAPAS_B200_ERR_UNSUPPORTED;
+}
 int m2l_fp64(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_fp64_P) }
 
 static int m2l_pairs_dispatch(tapas_b200_ctx *ctx) { TB_DISPATCH_P(ctx->P, m2l_pairs_P) }

@@ -12,6 +12,12 @@ int upward_fp32_p2m(tapas_b200_ctx *ctx, int P);
 // the whole tree from the leaves' M (order ctx->P).
 int p2m_only(tapas_b200_ctx *ctx, int P, bool fp32);
 int m2m_only(tapas_b200_ctx *ctx);
+// FP64 M2M level GEMMs of parent levels max_levels - 1 .. 0 only (deepest
+// first), order ctx->P; builds the level operators for the current tree.
+int fp64_m2m_levels(tapas_b200_ctx *ctx, int max_levels);
+// The plain FP64 form's M2L: one FP64 GEMM per offset class (classes in key
+// order, so every target's sum has a fixed order), the rare classes' pairs by
+// the warp-per-target FP64 kernel.
 int m2l_fp64(tapas_b200_ctx *ctx);
 // L zeroed, then the FP64 M2L of the pairs at list indices pairs[0..npairs)
 // added into it (atomics: the order of a target's sums is not fixed).

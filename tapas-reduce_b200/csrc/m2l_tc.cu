@@ -46,7 +46,9 @@ constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor
 constexpr int kNTile = 128;        // pairs per tile (MMA N)
 constexpr int kOffBias = 8192;
 
-template <int P>
+// kDense: every M-tile reads every K-chunk (the M2M operators of the tree
+// translations, whose zero structure differs from M2L's).
+template <int P, bool kDense = false>
 struct TcShape {
   static constexpr int NT = P * (P + 1) / 2;
   static constexpr int K = 2 * NT;                    // real dimension
@@ -80,6 +82,7 @@ struct TcShape {
     return j;
   }
   static constexpr int kc_need(int mt) {
+    if (kDense) return NKC;
     const int c = ((P - jmin(mt)) * (P - jmin(mt) + 1) + KC - 1) / KC;
     return c < NKC ? c : NKC;
   }
@@ -624,10 +627,10 @@ __device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volat
 // (hi*hi, lo*hi, hi*lo) into TMEM columns dcol + [mt*128, mt*128+128).
 // a_hi/a_lo point at the chunk's operator rows (core-matrix layout), b_hi/b_lo
 // at the chunk's 128 multipole rows.
-template <int P>
+template <int P, bool kDense = false>
 __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, uint32_t a_lo,
                                                  uint32_t b_hi, uint32_t b_lo, int kc) {
-  using S = TcShape<P>;
+  using S = TcShape<P, kDense>;
   const int mcnt = S::mcount(kc);  // M-tiles with nonzero operator entries in this chunk
   // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
@@ -679,14 +682,14 @@ constexpr int kThreadsTc = 32 * 17;
 //    two TMEM buffers the epilogue of tile i overlaps the MMAs of tile i+1.
 // Every wait is bounded and also gives up when another role has aborted; the
 // CTA then drains its copies and its MMAs before freeing TMEM.
-template <int P>
+template <int P, bool kDense = false>
 __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
     const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
     const float *__restrict__ ops_lo, const float *__restrict__ Mt_hi,
     const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err,
     long long wait_limit) {
-  using S = TcShape<P>;
+  using S = TcShape<P, kDense>;
   constexpr int NS = S::NS;
   constexpr int NB = S::TBUF;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -835,7 +838,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
           float *sA_lo = sA_hi + S::MP * S::KC;
           float *sB_hi = sA_lo + S::MP * S::KC;
           float *sB_lo = sB_hi + kNTile * S::KC;
-          issue_chunk_mmas<P>(dcol, smem_u32(sA_hi), smem_u32(sA_lo), smem_u32(sB_hi),
+          issue_chunk_mmas<P, kDense>(dcol, smem_u32(sA_hi), smem_u32(sA_lo), smem_u32(sB_hi),
                               smem_u32(sB_lo), kc);
           umma_commit(&empty[st]);
         }
@@ -1100,9 +1103,11 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   // 4. normalised multipoles, zeroed normalised locals
   TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));  // hi rows, then lo rows
   TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
-  normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
-      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP);
-  TB_LAUNCH_CHECK(ctx);
+  if (!T.mt_ready) {  // the mixed upward pass leaves them ready
+    normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
+        C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP);
+    TB_LAUNCH_CHECK(ctx);
+  }
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
   setup_timer.reset();
   // 5. FP64 part (rare classes) writes L; the GEMM adds into Lt
@@ -1136,7 +1141,299 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   return TAPAS_B200_OK;
 }
 
+// ---------------------------------------------------------------------------
+// M2M of the mixed form at the deepest levels, on the tensor cores.  With M_n
+// scaled by w^-n, a child's offset from its parent is +-1/2 child width per
+// axis at every level, so the M2M (ex/LaplaceSphericalCPU_tapas.h:165-206) has
+// eight level-independent operators: Mt_parent(j) = sum 2^-j T_o Mt_child.  A
+// level is then one GEMM launch over its (parent, child) pairs grouped by
+// octant, the dense form of the M2L kernel.
+// Only the deepest kTcUpLevels parent levels (and never levels 0 ..
+// kFp64TreeLevels - 1) run on the tensor cores; the others stay FP64 (level
+// GEMMs).  A split-TF32 translation keeps ~2^-22 of its input.  For the M2M
+// that is harmless (the M2L reads the multipoles in the same split form; on a
+// 16M-body sphere surface at P = 15 the tensor-core M2M moved the potential
+// error by 0.3%), and the deepest three parent levels hold nearly all of a
+// surface tree's cells.  The L2L stays FP64: it carries the whole local
+// expansion of every ancestor, so a split-TF32 error there compounds down the
+// chain and reaches the potential in full (tensor-core L2L on the deepest three
+// parent levels raised the same case's error from 6.7e-7 to 9.2e-7, 4.7e-7 of
+// it truncation).
+// ---------------------------------------------------------------------------
+constexpr int kFp64TreeLevels = 4;
+constexpr int kTcUpLevels = 3;
+constexpr int kTreeShift = 32;  // tree pair list entries: target << 32 | source
+
+// M2M operator classes o (octant o), each split into TF32 hi + lo in the
+// GEMM's layout.  child0: the first child of any non-leaf cell; the offsets
+// are its octants' centre offsets in child widths (exact: +-1/2).
+template <int P>
+__global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict__ cparent,
+                                                      const double *__restrict__ ccen,
+                                                      const double *__restrict__ cmin,
+                                                      const double *__restrict__ cmax,
+                                                      int64_t child0, float *__restrict__ ops_hi,
+                                                      float *__restrict__ ops_lo) {
+  using S = TcShape<P>;
+  __shared__ cd Y[P * P];
+  __shared__ unsigned char deg[S::NT], ord[S::NT];
+  const int o = blockIdx.x;
+  const int64_t c = child0 + o;
+  const int p = cparent[c];
+  const double wc = cmax[3 * c] - cmin[3 * c];
+  double d[3];
+  for (int k = 0; k < 3; k++) d[k] = (ccen[3 * p + k] - ccen[3 * c + k]) / wc;  // parent - child
+  const Sph sp = sph_of(d[0], d[1], d[2]);
+  if (threadIdx.x < P) multipole_column<P>(threadIdx.x, sp.r, sp.x, sp.y, sp.ei, Y);
+  for (int t = threadIdx.x; t < S::NT; t += blockDim.x) {
+    int j, k;
+    jk_of(t, j, k);
+    deg[t] = (unsigned char)j;
+    ord[t] = (unsigned char)k;
+  }
+  __syncthreads();
+  float *hi = ops_hi + (size_t)o * S::MP * S::KP;
+  float *lo = ops_lo + (size_t)o * S::MP * S::KP;
+  for (int idx = threadIdx.x; idx < (S::MP / 2) * (S::KP / 2); idx += blockDim.x) {
+    const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // target / source coefficient
+    cd a{0, 0}, b{0, 0};  // target += a * source + b * conj(source)
+    if (2 * to < S::K && 2 * ti < S::K) {
+      const int j = deg[to], k = ord[to], jp = deg[ti], kp = ord[ti];
+      const int n = j - jp;
+      if (n >= 0) {
+        if (kp >= 1) {
+          const int m = k - kp;
+          if (m >= -n && m <= n)
+            a = scal(((m >= 0) ? 1.0 : oddeven(m)) * oddeven(n), Y[n * n + n - m]);
+        }
+        const int m = k + kp;
+        if (m <= n) b = scal(oddeven(k + n + m), Y[n * n + n - m]);
+      }
+      const double sc = ldexp(1.0, -j);
+      a = scal(sc, a);
+      b = scal(sc, b);
+    }
+    // [row re/im][column re/im] of the real 2 x 2 block
+    const double v[4] = {a.x + b.x, b.y - a.y, a.y + b.y, a.x - b.x};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float f = (float)v[e];
+      const float h = tf32_round(f);
+      const size_t off = op_offset<P>(2 * to + (e >> 1), 2 * ti + (e & 1));
+      hi[off] = h;
+      lo[off] = tf32_round(f - h);
+    }
+  }
+}
+
+// The (parent, child) pairs of one level's M2M, octant-major: entry o * np + i
+// is parent i's octant o.  c0: the level's first child.
+__global__ void tree_pairs(int64_t c0, int64_t np, const int32_t *__restrict__ cparent,
+                           uint64_t *__restrict__ list) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 8 * np;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = e / np, i = e - o * np;
+    const uint64_t child = (uint64_t)(c0 + 8 * i + o), parent = (uint64_t)cparent[c0 + 8 * i];
+    list[e] = parent << kTreeShift | child;
+  }
+}
+
+__global__ void iota_u32(uint32_t *__restrict__ v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+
+// After a level's M2M: per parent (one warp each) its normalised FP32 sum A
+// becomes the GEMM's split input row and its FP64 multipoles (A w^n).
+template <int P>
+__global__ void __launch_bounds__(256) finish_parents(int64_t c0, int64_t np,
+                                                      const int32_t *__restrict__ cparent,
+                                                      const double *__restrict__ cmin,
+                                                      const double *__restrict__ cmax,
+                                                      const float *__restrict__ acc,
+                                                      float *__restrict__ Mt_hi,
+                                                      float *__restrict__ Mt_lo,
+                                                      double2 *__restrict__ M) {
+  using S = TcShape<P>;
+  __shared__ double pw[8][P];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int64_t nw = (int64_t)gridDim.x * 8;
+  for (int64_t i = (int64_t)blockIdx.x * 8 + wi; i < np; i += nw) {
+    const int64_t p = cparent[c0 + 8 * i];
+    __syncwarp();
+    if (lane < P) pw[wi][lane] = pow(cmax[3 * p] - cmin[3 * p], lane);
+    __syncwarp();
+    for (int kk = lane; kk < S::KP; kk += 32) {
+      const float v = acc[p * S::KP + kk];
+      const float h = tf32_round(v);
+      Mt_hi[p * S::KP + kk] = h;
+      Mt_lo[p * S::KP + kk] = tf32_round(v - h);
+    }
+    for (int t = lane; t < S::NT; t += 32) {
+      int j, k;
+      jk_of(t, j, k);
+      const float2 a = *reinterpret_cast<const float2 *>(acc + p * S::KP + 2 * t);
+      M[p * S::NT + t] = make_double2((double)a.x * pw[wi][j], (double)a.y * pw[wi][j]);
+    }
+  }
+}
+
+// One level's M2M GEMM: the children's split rows translated into the parents'
+// normalised rows of out (FP32, accumulated).
+template <int P>
+int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *B_hi,
+                    const float *B_lo, float *out) {
+  using S = TcShape<P, true>;
+  cudaStream_t s = ctx->stream;
+  auto &T = ctx->tc;
+  tree_pairs<<<grid_for(8 * np, 256), 256, 0, s>>>(c0, np, ctx->cparent.p, T.tree_list.p);
+  TB_LAUNCH_CHECK(ctx);
+  std::vector<TileItem> items;
+  items.reserve((size_t)(8 * ((np + kNTile - 1) / kNTile)));
+  for (int o = 0; o < 8; o++)
+    for (int64_t st = 0; st < np; st += kNTile) {
+      TileItem it;
+      it.cls = o;
+      it.start = (int32_t)(o * np + st);
+      it.len = (int32_t)std::min<int64_t>(kNTile, np - st);
+      it.pad = 0;
+      items.push_back(it);
+    }
+  const int64_t nitems = (int64_t)items.size();
+  TB_CUDA(ctx, T.tree_items.ensure((size_t)nitems * sizeof(TileItem) / 16 + 1, s));
+  TB_CUDA(ctx, ctx->pinned.ensure(sizeof(TileItem) * (size_t)nitems + 256));
+  memcpy(ctx->pinned.p, items.data(), sizeof(TileItem) * (size_t)nitems);
+  TB_CUDA(ctx, cudaMemcpyAsync(T.tree_items.p, ctx->pinned.p, sizeof(TileItem) * (size_t)nitems,
+                               cudaMemcpyHostToDevice, s));
+  TB_CUDA(ctx, cudaStreamSynchronize(s));  // the pinned staging buffer is reused
+  static_assert(S::SMEM <= 227 * 1024 - 4096, "shared memory");
+  TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+  const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
+  m2l_tc_kernel<P, true><<<grid, kThreadsTc, S::SMEM, s>>>(
+      reinterpret_cast<const TileItem *>(T.tree_items.p), nitems, T.iota.p, T.tree_list.p,
+      kTreeShift, T.ops_tr_hi.p, T.ops_tr_lo.p, B_hi, B_lo, out, T.err.p, ctx->tc_wait_limit);
+  TB_LAUNCH_CHECK(ctx);
+  return TAPAS_B200_OK;
+}
+
+// Tree levels: parents at level l have their 8 children at
+// [level_off[l + 1] + 8 i, ...); the number of levels with parents.
+int tree_parent_levels(const tapas_b200_ctx *ctx) {
+  int nlev = 0;
+  for (int l = 0; l + 2 < (int)ctx->level_off.size(); l++) {
+    if (ctx->level_off[l + 2] <= ctx->level_off[l + 1]) break;
+    nlev = l + 1;
+  }
+  return nlev;
+}
+
+// The first parent level of the tensor-core M2M (levels above it: FP64).
+int first_tc_tree_level(int nlev) { return std::max(kFp64TreeLevels, nlev - kTcUpLevels); }
+
+// Pair lists, operators and the abort flag of the tree GEMMs; only for trees
+// with parent levels from kFp64TreeLevels on (level 1 exists).
+template <int P>
+int tc_tree_prepare(tapas_b200_ctx *ctx) {
+  using S = TcShape<P>;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  auto &T = ctx->tc;
+  TB_CUDA(ctx, T.tree_list.ensure((size_t)C + 8, s));
+  if (T.iota_n < C) {
+    TB_CUDA(ctx, T.iota.ensure((size_t)C + 8, s));
+    iota_u32<<<grid_for(C + 8, 256), 256, 0, s>>>(T.iota.p, C + 8);
+    TB_LAUNCH_CHECK(ctx);
+    T.iota_n = C;
+  }
+  if (T.tr_P != P) {
+    const size_t opsz = (size_t)S::MP * S::KP * 8;
+    TB_CUDA(ctx, T.ops_tr_hi.ensure(opsz, s));
+    TB_CUDA(ctx, T.ops_tr_lo.ensure(opsz, s));
+    build_tree_ops<P><<<8, 256, 0, s>>>(ctx->cparent.p, ctx->ccen.p, ctx->cmin.p,
+                                                  ctx->cmax.p, ctx->level_off[1], T.ops_tr_hi.p,
+                                                  T.ops_tr_lo.p);
+    TB_LAUNCH_CHECK(ctx);
+    T.tr_P = P;
+  }
+  TB_CUDA(ctx, T.err.ensure(4, s));
+  TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
+  return TAPAS_B200_OK;
+}
+
+int check_tc_abort(tapas_b200_ctx *ctx, const char *what) {
+  int *h = reinterpret_cast<int *>(ctx->pinned.p);
+  TB_CUDA(ctx, cudaMemcpyAsync(h, ctx->tc.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[0]) {
+    set_error(ctx, "%s tensor-core kernel: a bounded wait on an MMA completion gave up", what);
+    return TAPAS_B200_ERR_TIMEOUT;
+  }
+  return TAPAS_B200_OK;
+}
+
+// Mixed upward after the FP32 P2M (leaf M in FP64): normalised split rows of
+// every cell, tensor-core M2M for the deepest parent levels (from
+// first_tc_tree_level, deepest first), FP64 level GEMMs above, the upper
+// cells' rows.  Leaves ctx->M (FP64) and the M2L's input rows (tc.Mt) complete.
+template <int P>
+int tc_tree_upward_P(tapas_b200_ctx *ctx) {
+  using S = TcShape<P>;
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  auto &T = ctx->tc;
+  TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));
+  TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
+  float *mt_hi = T.Mt.p, *mt_lo = T.Mt.p + (size_t)C * S::KP;
+  normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
+      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt_hi, mt_lo);
+  TB_LAUNCH_CHECK(ctx);
+  const int nlev = tree_parent_levels(ctx), l0 = first_tc_tree_level(nlev);
+  if (nlev > l0) {
+    TB_TRY(tc_tree_prepare<P>(ctx));
+    TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
+    for (int l = nlev - 1; l >= l0; l--) {
+      const int64_t c0 = ctx->level_off[l + 1], np = (ctx->level_off[l + 2] - c0) / 8;
+      if (np <= 0) continue;
+      TB_TRY(tree_level_gemm<P>(ctx, c0, np, mt_hi, mt_lo, T.Lt.p));
+      finish_parents<P><<<grid_for(np, 8, ctx->num_sms * 8), 256, 0, s>>>(
+          c0, np, ctx->cparent.p, ctx->cmin.p, ctx->cmax.p, T.Lt.p, mt_hi, mt_lo, ctx->M.p);
+      TB_LAUNCH_CHECK(ctx);
+    }
+    TB_TRY(check_tc_abort(ctx, "M2M"));
+  }
+  TB_TRY(fp64_m2m_levels(ctx, l0));
+  // rows of the cells the FP64 levels produced (levels 0 .. l0 - 1)
+  const int64_t ctop =
+      std::min<int64_t>(C, ctx->level_off[std::min<size_t>(l0, ctx->level_off.size() - 1)]);
+  if (ctop > 0) {
+    normalize_M<P><<<grid_for(ctop, 8, ctx->num_sms * 8), 256, 0, s>>>(
+        ctop, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt_hi, mt_lo);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  T.mt_ready = true;
+  return TAPAS_B200_OK;
+}
+
+#define TB_TC_DISPATCH(FN)                                                                   \
+  switch (ctx->P) {                                                                          \
+    case 4: return FN<4>(ctx);   case 5: return FN<5>(ctx);   case 6: return FN<6>(ctx);     \
+    case 7: return FN<7>(ctx);   case 8: return FN<8>(ctx);   case 9: return FN<9>(ctx);     \
+    case 10: return FN<10>(ctx); case 11: return FN<11>(ctx); case 12: return FN<12>(ctx);   \
+    case 13: return FN<13>(ctx); case 14: return FN<14>(ctx); case 15: return FN<15>(ctx);   \
+    case 16: return FN<16>(ctx);                                                             \
+    default: break;                                                                          \
+  }
+
 }  // namespace
+
+int tc_tree_upward(tapas_b200_ctx *ctx) {
+  TB_TC_DISPATCH(tc_tree_upward_P)
+  // P = 2, 3: the FP64 level GEMMs do every level
+  ctx->tc.mt_ready = false;
+  return fp64_m2m_levels(ctx, 1 << 20);
+}
 
 int m2l_tensorcore(tapas_b200_ctx *ctx) {
   switch (ctx->P) {

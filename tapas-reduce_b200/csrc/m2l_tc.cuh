@@ -8,10 +8,12 @@ namespace tb {
 // enough pairs on the tensor cores, the remainder with the FP64 kernel.
 int m2l_tensorcore(tapas_b200_ctx *ctx);
 
-// The plain FP64 form's M2L: one FP64 GEMM per offset class (classes in key
-// order, so every target's sum has a fixed order), the rare classes' pairs by
-// the warp-per-target FP64 kernel (m2l_gemm64.cu).
-int m2l_fp64_gemm(tapas_b200_ctx *ctx);
+// The mixed form's M2M, after its FP32 P2M: tensor-core GEMMs per level over
+// (parent, child) pairs grouped by octant with level-independent,
+// width-normalised operators at the deepest three parent levels below level
+// 3, FP64 level GEMMs above them.  Completes ctx->M and the M2L's input rows.
+// (The mixed form's L2L is the FP64 one.)
+int tc_tree_upward(tapas_b200_ctx *ctx);
 
 // Result of the offset classification of the current M2L list.
 struct M2LClassInfo {

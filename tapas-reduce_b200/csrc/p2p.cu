@@ -359,6 +359,9 @@ __device__ __forceinline__ void mixed_tile(
   const int g = lane / L, tl = lane - g * L;
   const bool active = g < G;
   const int gs = active ? g : kStage;  // idle lanes skip the source loop
+  // a source body this far from the target leaf's centre (max norm) is far;
+  // the margin covers the FP32 rounding of the test itself
+  const float far_body = (float)(tw * (5.0 / 6.0)) * (1.0f + 1e-6f);
   float txh[kR], tyh[kR], tzh[kR], txl[kR], tyl[kR], tzl[kR];
   float ps[kR], pc[kR], xs[kR], xc[kR], ys[kR], yc[kR], zs[kR], zc[kR];
   float tp[kR], tx[kR], ty[kR], tz[kR];
@@ -411,18 +414,40 @@ __device__ __forceinline__ void mixed_tile(
     while (j < nbat) {
       const int cnt = min(kStage, ns_j - ch);
       __syncwarp();
-      const bool far = meta[j].far != 0;
-      if (lane < cnt) {
+      // Far bodies first (single floats), then near ones (hi, lo).  A body is
+      // far when its whole leaf is, or when its max-norm distance from the
+      // target leaf's centre is at least 5/6 of the leaf width: then every
+      // target is >= D - tw/2 away while the coordinates are <= D and tw/2, so
+      // one rounding is <= 2^-24 (D + tw/2) / (D - tw/2) <= 4 * 2^-24 of a
+      // separation, the leaf rule's bound.
+      int nfar;
+      {
         const LeafMeta &m = meta[j];
-        float ex, ey, ez;
-        const float ax = two_sum(ph.x, m.hx, ex), ay = two_sum(ph.y, m.hy, ey),
-                    az = two_sum(ph.z, m.hz, ez);
-        const float lx = ex + (pl.x + m.lx), ly = ey + (pl.y + m.ly), lz = ez + (pl.z + m.lz);
-        if (far) {  // one float per coordinate, rounded once
-          ss[wi][lane].hi = make_float4(ax + lx, ay + ly, az + lz, ph.w);
-        } else {
-          ss[wi][lane].hi = make_float4(ax, ay, az, ph.w);
-          ss[wi][lane].lo = make_float4(lx, ly, lz, 0.f);
+        float ex = 0.f, ey = 0.f, ez = 0.f, ax = 0.f, ay = 0.f, az = 0.f, lx = 0.f, ly = 0.f,
+              lz = 0.f;
+        bool farb = true;
+        if (lane < cnt) {
+          ax = two_sum(ph.x, m.hx, ex);
+          ay = two_sum(ph.y, m.hy, ey);
+          az = two_sum(ph.z, m.hz, ez);
+          lx = ex + (pl.x + m.lx);
+          ly = ey + (pl.y + m.ly);
+          lz = ez + (pl.z + m.lz);
+          if (!m.far)
+            farb = fmaxf(fabsf(ax + lx), fmaxf(fabsf(ay + ly), fabsf(az + lz))) >= far_body;
+        }
+        const unsigned valid = cnt >= 32 ? 0xffffffffu : ((1u << cnt) - 1u);
+        const unsigned fm = __ballot_sync(0xffffffffu, farb) & valid;
+        const unsigned below = (1u << lane) - 1u;
+        nfar = __popc(fm);
+        if (lane < cnt) {
+          if (farb) {  // one float per coordinate, rounded once
+            ss[wi][__popc(fm & below)].hi = make_float4(ax + lx, ay + ly, az + lz, ph.w);
+          } else {
+            const int k = nfar + __popc(~fm & valid & below);
+            ss[wi][k].hi = make_float4(ax, ay, az, ph.w);
+            ss[wi][k].lo = make_float4(lx, ly, lz, 0.f);
+          }
         }
       }
       __syncwarp();
@@ -441,11 +466,11 @@ __device__ __forceinline__ void mixed_tile(
           pl = rel_lo[b0 + ch2 + lane];
         }
       }
-      if (far) {
-        // separated leaves: plain FP32 coordinates in the target frame (relative
+      {
+        // far bodies: plain FP32 coordinates in the target frame (relative
         // error of a separation <= ~2.4e-7), no r = 0 case
 #pragma unroll 2
-        for (int k = gs; k < cnt; k += G) {
+        for (int k = gs; k < nfar; k += G) {
           const float4 bh = ss[wi][k].hi;
 #pragma unroll
           for (int r = 0; r < kR; r++) {
@@ -460,11 +485,12 @@ __device__ __forceinline__ void mixed_tile(
             tz[r] = fmaf(dz, qr3, tz[r]);
           }
         }
-      } else {
-        // touching or nearby leaves: separations from (hi, lo) coordinates
+      }
+      if (nfar < cnt) {
+        // near bodies: separations from (hi, lo) coordinates
         // two sources in flight: their rsqrt latencies overlap
 #pragma unroll 2
-        for (int k = gs; k < cnt; k += G) {
+        for (int k = nfar + gs; k < cnt; k += G) {
           const float4 bh = ss[wi][k].hi;
           const float4 bl = ss[wi][k].lo;
 #pragma unroll

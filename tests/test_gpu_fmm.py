@@ -420,12 +420,44 @@ def test_tensorcore_m2l_wait_timeout_is_a_status(tb, ctx):
     assert rel.max() < 2e-5
 
 
+@pytest.mark.parametrize("P", [6, 12, 16])
+def test_mixed_tree_translations_per_cell(P, tb, ctx):
+    """The mixed form's tree translations (M2M: split-TF32 tensor-core GEMMs
+    with level-independent operators on the deepest three parent levels below
+    level 3, FP64 level GEMMs above them; L2L: FP64) on a deep tree, per cell
+    against the FP64 form: multipoles within 1e-6 of
+    the cell's multipoles of |q| (see below), local expansions after the
+    downward pass within 5e-5 of the FP64 ones."""
+    x, y, z, q = tb.datasets.make("two_gaussians", 200000, 19)
+    ctx.partition(x, y, z, np.abs(q), ncrit=32)
+    ctx.upward(P, tb.FP64)
+    Mabs, _ = ctx.expansions()
+    assert ctx.tree_info()["max_depth"] >= 8  # levels below the FP64 ones exist
+    out = {}
+    for prec in (tb.FP64, tb.MIXED):
+        ctx.partition(x, y, z, q, ncrit=32)
+        ctx.upward(P, prec)
+        ctx.traverse(0.4, 0, prec)
+        ctx.downward(prec)
+        out[prec] = ctx.expansions()
+    (M64, L64), (Mmx, Lmx) = out[tb.FP64], out[tb.MIXED]
+    scale = np.linalg.norm(Mabs, axis=1)
+    ok = scale > 0
+    relM = np.linalg.norm(Mmx[ok] - M64[ok], axis=1) / scale[ok]
+    assert relM.max() < 1e-6, relM.max()
+    nrm = np.linalg.norm(L64, axis=1)
+    ne = (ctx.cells()["nb"] > 0) & (nrm > 0)
+    relL = np.linalg.norm(Lmx[ne] - L64[ne], axis=1) / nrm[ne]
+    assert relL.max() < 5e-5, (relL.max(), np.median(relL))
+
+
 @pytest.mark.parametrize("P", [4, 10, 16])
 @pytest.mark.parametrize("dist", ["sphere_surface", "two_gaussians"])
 def test_fp32_p2m_per_cell(P, dist, tb, ctx):
     """The mixed form's P2M (FP32 terms in units of the leaf width, FP32 warp
-    reduce-scatter, FP64 sums over body chunks) followed by the FP64 M2M,
-    against the FP64 upward pass, per cell.  An FP32 term rounds to ~6e-8 of
+    reduce-scatter, FP64 sums over body chunks) followed by its M2M (FP64 at
+    the top levels, split-TF32 tensor cores below), against the FP64 upward
+    pass, per cell.  An FP32 term rounds to ~6e-8 of
     itself, so the error of a cell's M is bounded by its scale without
     cancellation: ||M_mixed - M_fp64|| <= 1e-6 ||M_|q|||, M_|q| the FP64
     multipoles of the charges' magnitudes.  (Where zero-mean charges cancel,
