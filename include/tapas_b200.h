@@ -39,7 +39,7 @@ typedef enum {
   TAPAS_B200_ERR_NOMEM = -3,       /* device or host allocation failed         */
   TAPAS_B200_ERR_STATE = -4,       /* call out of order (e.g. upward before partition) */
   TAPAS_B200_ERR_CAPACITY = -5,    /* a device work queue hit its bound        */
-  TAPAS_B200_ERR_UNSUPPORTED = -6, /* e.g. mutual=1, expansion order outside 2..16 */
+  TAPAS_B200_ERR_UNSUPPORTED = -6, /* e.g. expansion order outside 2..16         */
   TAPAS_B200_ERR_TIMEOUT = -7      /* a bounded device wait gave up            */
 } tapas_b200_status;
 
@@ -50,7 +50,9 @@ enum {
   TAPAS_B200_FP64 = 0,  /* plain FP64 everywhere (the reference's FP64 build)          */
   TAPAS_B200_MIXED = 1  /* FP32 compensated P2P; FP32 P2M and L2P in units of the leaf
                            width; split-TF32 tensor-core M2L (FP64 for rare offset
-                           classes); FP64 M2M/L2L; FP64 sums and outputs               */
+                           classes); split-TF32 tensor-core M2M at the deepest three
+                           parent levels below level 3, FP64 M2M above them; FP64
+                           L2L; FP64 sums and outputs                                 */
 };
 
 /* Output order of per-body results. */
