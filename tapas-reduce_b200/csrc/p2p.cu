@@ -48,6 +48,7 @@ constexpr int kMaxR = 3;     // FP64: targets per lane, leaves up to 96 bodies p
 // mixed kernel: 4-warp CTAs, 4 per SM (<= 128 registers, 16 warps per SM), up to
 // 3 targets per lane (leaves of more than 96 bodies take two passes)
 constexpr int kMixedWarps = 4;
+constexpr int kMixedMaxR = 3;  // most targets per lane of the mixed kernel
 constexpr int kMixedThreads = 32 * kMixedWarps;
 
 // ---------------------------------------------------------------------------
@@ -285,6 +286,14 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
   sum = t;
 }
 
+// The same on a (sum, compensation) pair held in shared memory.
+__device__ __forceinline__ void kahan_add_sm(float &sum_sm, float &comp_sm, float v) {
+  float sum = sum_sm, comp = comp_sm;
+  kahan_add(sum, comp, v);
+  sum_sm = sum;
+  comp_sm = comp;
+}
+
 // a + b = s + e exactly (Knuth's TwoSum)
 __device__ __forceinline__ float two_sum(float a, float b, float &e) {
   const float s = __fadd_rn(a, b);
@@ -355,7 +364,8 @@ __device__ __forceinline__ void mixed_tile(
     const double *__restrict__ ccen, const double *__restrict__ cmin,
     const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
     const float4 *__restrict__ rel_lo, SrcRec (*ss)[kStage],
-    LeafMeta (*mt)[32], double4 (*red)[32], double4 *__restrict__ out) {
+    LeafMeta (*mt)[32], double4 (*red)[32], float (*kc)[kMixedMaxR][8][32],
+    double4 *__restrict__ out) {
   const int g = lane / L, tl = lane - g * L;
   const bool active = g < G;
   const int gs = active ? g : kStage;  // idle lanes skip the source loop
@@ -363,8 +373,11 @@ __device__ __forceinline__ void mixed_tile(
   // the margin covers the FP32 rounding of the test itself
   const float far_body = (float)(tw * (5.0 / 6.0)) * (1.0f + 1e-6f);
   float txh[kR], tyh[kR], tzh[kR], txl[kR], tyl[kR], tzl[kR];
-  float ps[kR], pc[kR], xs[kR], xc[kR], ys[kR], yc[kR], zs[kR], zc[kR];
   float tp[kR], tx[kR], ty[kR], tz[kR];
+  // the Kahan (sum, compensation) pairs of pot, ax, ay, az per target live in
+  // the warp's shared-memory slice (touched once per source leaf), which keeps
+  // the kernel at 6 CTAs per SM
+  float(*kw)[8][32] = kc[wi];
 #pragma unroll
   for (int r = 0; r < kR; r++) {
     const int t = tl + L * r;
@@ -373,7 +386,8 @@ __device__ __forceinline__ void mixed_tile(
     const float4 l = v ? rel_lo[tb0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
     txh[r] = h.x; tyh[r] = h.y; tzh[r] = h.z;
     txl[r] = l.x; tyl[r] = l.y; tzl[r] = l.z;
-    ps[r] = pc[r] = xs[r] = xc[r] = ys[r] = yc[r] = zs[r] = zc[r] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) kw[r][k][lane] = 0.f;
     tp[r] = tx[r] = ty[r] = tz[r] = 0.f;
   }
   LeafMeta *const meta = mt[wi];
@@ -513,10 +527,10 @@ __device__ __forceinline__ void mixed_tile(
         // one source leaf summed in FP32: Kahan-add it into the target's sums
 #pragma unroll
         for (int r = 0; r < kR; r++) {
-          kahan_add(ps[r], pc[r], tp[r]);
-          kahan_add(xs[r], xc[r], tx[r]);
-          kahan_add(ys[r], yc[r], ty[r]);
-          kahan_add(zs[r], zc[r], tz[r]);
+          kahan_add_sm(kw[r][0][lane], kw[r][1][lane], tp[r]);
+          kahan_add_sm(kw[r][2][lane], kw[r][3][lane], tx[r]);
+          kahan_add_sm(kw[r][4][lane], kw[r][5][lane], ty[r]);
+          kahan_add_sm(kw[r][6][lane], kw[r][7][lane], tz[r]);
           tp[r] = tx[r] = ty[r] = tz[r] = 0.f;
         }
       }
@@ -525,10 +539,13 @@ __device__ __forceinline__ void mixed_tile(
       ns_j = ns2;
     }
   }
+  __syncwarp();
 #pragma unroll
   for (int r = 0; r < kR; r++) {
-    double4 v = make_double4((double)ps[r] - (double)pc[r], -((double)xs[r] - (double)xc[r]),
-                             -((double)ys[r] - (double)yc[r]), -((double)zs[r] - (double)zc[r]));
+    const float *k = &kw[r][0][lane];
+    double4 v = make_double4((double)k[0] - (double)k[32], -((double)k[64] - (double)k[96]),
+                             -((double)k[128] - (double)k[160]),
+                             -((double)k[192] - (double)k[224]));
     if (G > 1) {
       __syncwarp();
       red[wi][lane] = v;
@@ -553,9 +570,11 @@ __global__ void __launch_bounds__(kMixedThreads, kBlocks) p2p_mixed_kernel(
     const double *__restrict__ ccen, const double *__restrict__ cmin,
     const double *__restrict__ cmax, const float4 *__restrict__ rel_hi,
     const float4 *__restrict__ rel_lo, double *__restrict__ trg, double *__restrict__ part) {
+  static_assert(kMaxRm <= kMixedMaxR, "targets per lane");
   __shared__ SrcRec ss[kMixedWarps][kStage];
   __shared__ LeafMeta mt[kMixedWarps][32];
   __shared__ double4 red[kMixedWarps][32];
+  __shared__ float kc[kMixedWarps][kMixedMaxR][8][32];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   for (;;) {
     const int w = next_leaf(counter, lane);
@@ -574,7 +593,7 @@ __global__ void __launch_bounds__(kMixedThreads, kBlocks) p2p_mixed_kernel(
       mixed_shape<kMaxRm>(nt, R, L, G);
 #define TB_MIXED_TILE(RR)                                                                     \
   mixed_tile<RR>(lane, wi, tb0 + tbase, nt, L, G, e0, e1, tcx, tcy, tcz, tw, list, src_mask, \
-                 cbeg, cnb, ccen, cmin, cmax, rel_hi, rel_lo, ss, mt, red, out + tbase)
+                 cbeg, cnb, ccen, cmin, cmax, rel_hi, rel_lo, ss, mt, red, kc, out + tbase)
       if (R == 1) TB_MIXED_TILE(1);
       else if (R == 2) TB_MIXED_TILE(2);
       else if (kMaxRm == 3 || R == 3) TB_MIXED_TILE(3);
@@ -703,9 +722,9 @@ int p2p_mixed(tapas_b200_ctx *ctx) {
   TB_LAUNCH_CHECK(ctx);
   TB_TRY(p2p_items(ctx));
   const uint64_t mask = (1ull << ctx->list_shift) - 1;
-  // up to 3 targets per lane at 16 warps per SM: measured faster than 4 targets at
-  // 12 warps in most sphere, cube and Plummer sets of 1M-16M bodies, ncrit 16-128
-  p2p_mixed_kernel<3, 4><<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
+  // up to 3 targets per lane; the Kahan pairs in shared memory keep the kernel
+  // at 80 registers, 24 warps per SM
+  p2p_mixed_kernel<3, 6><<<p2p_grid(ctx, kMixedWarps), kMixedThreads, 0, s>>>(
       ctx->p2p_order.p, ctx->p2p_nitems, ctx->p2p_counter.p,
       reinterpret_cast<const WorkItem *>(ctx->p2p_items.p), ctx->p2p.p, mask, ctx->cbeg.p,
       ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p, ctx->rel4.p, ctx->rel_lo.p,
