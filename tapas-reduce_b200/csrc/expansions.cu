@@ -172,7 +172,7 @@ __device__ __forceinline__ float warp_reduce_scatter16f(float (&buf)[16], int la
 // is more than 1e-7 of M itself (up to ~2e-5 of it measured), which the final
 // potential does not feel (it sums the same terms the cancellation removed).
 template <int P>
-__global__ void __launch_bounds__(kThreads) p2m32_kernel(
+__global__ void __launch_bounds__(kThreads, 6) p2m32_kernel(
     const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
     const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
     const double *__restrict__ cmin, const double *__restrict__ cmax,
@@ -566,6 +566,9 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
     float2 eim = make_float2(1.f, 0.f);
 #pragma unroll
     for (int m = 0; m < P; m++) {
+      // keeps the compiler from hoisting every column's shared-memory loads
+      // of L ahead of the loop (168 registers at P = 15 instead of 80)
+      asm volatile("" ::: "memory");
       float p = pn, p1 = pn;
       float rhon = rhom;
       float2 sa = make_float2(0.f, 0.f), sb = sa, sc = sa;

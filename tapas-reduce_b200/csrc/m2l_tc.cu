@@ -8,8 +8,8 @@
 // delta = depth_t - depth_s and the integer offset
 // D = (c_t - c_s) / (w_min / 2) (centres of cells are odd multiples of half
 // their width from the cube corner, so D is an integer vector).  Every M2L
-// pair of a class is then one column of a dense GEMM
-//     Lt[:, pairs] += T_class (K x K) * Mt[:, sources of pairs].
+// pair of a class is then one row of a dense GEMM
+//     Lt[targets of pairs, :] += Mt[sources of pairs, :] * T_class^T (K x K).
 //
 // Execution:
 //  1. classify: class key per M2L pair; stable radix sort of the pairs by key
@@ -21,15 +21,20 @@
 //     unit-width singular harmonics and split into TF32 hi + lo parts, laid
 //     out as K-major core matrices (8 rows x 16 bytes) ready for smem.
 //  4. GEMM kernel, warp-specialised: a CTA takes tiles of 128 pairs of one
-//     class; producer warps stream the operator's K chunks (bulk copies) and
-//     the sources' pre-split multipole rows (cp.async) through a 2-4 stage
-//     shared-memory ring; one thread issues tcgen05.mma kind::tf32 (M=128 rows
-//     of T per M-tile, N=128 pairs, K=8) three times per k-step (hi*hi +
-//     lo*hi + hi*lo: split-precision "3xTF32", FP32 accumulation in TMEM);
-//     epilogue warps read the finished accumulator with tcgen05.ld and add
-//     each column into its target's Lt with fire-and-forget reductions, while
-//     the next tile accumulates in the second TMEM buffer.  All hand-offs are
-//     mbarriers with bounded waits.
+//     class; producer warps stream the sources' FP32 multipole rows
+//     (cp.async, split into TF32 hi + lo in shared memory) and the operator's
+//     K chunks (bulk copies) through a shared-memory ring; one thread issues tcgen05.mma kind::tf32 (M=128
+//     pairs, N = the operator rows the chunk reaches, K=8) three times per
+//     k-step (hi*hi + lo*hi + hi*lo: split-precision "3xTF32", FP32
+//     accumulation in TMEM).  An output of degree j reads only sources of
+//     degree n < P - j, so with outputs in degree order the rows a K-chunk
+//     reaches are a prefix that shrinks along K: at P = 15 the chunks need
+//     976 operator rows in all instead of 15 x 240, which divides the MMA
+//     work and the operator bytes by 2.2.  Epilogue warps read a finished
+//     accumulator with tcgen05.ld (one pair per TMEM lane, 32 outputs per
+//     load) and add each pair's row into its target's Lt with vector
+//     fire-and-forget reductions, while the next tile accumulates in the
+//     second TMEM buffer.  All hand-offs are mbarriers with bounded waits.
 //  5. Lt is rescaled and added into the FP64 L.
 #include <algorithm>
 #include <optional>
@@ -46,50 +51,48 @@ constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor
 constexpr int kNTile = 128;        // pairs per tile (MMA N)
 constexpr int kOffBias = 8192;
 
-// kDense: every M-tile reads every K-chunk (the M2M operators of the tree
-// translations, whose zero structure differs from M2L's).
+// kDense: every K-chunk reaches every operator row (the M2M operators of the
+// tree translations, whose zero structure differs from M2L's).
 template <int P, bool kDense = false>
 struct TcShape {
   static constexpr int NT = P * (P + 1) / 2;
   static constexpr int K = 2 * NT;                    // real dimension
-  static constexpr int MT = (K + 127) / 128;          // M-tiles of 128 operator rows
-  static constexpr int MP = MT * 128;
-  // K chunk per stage: small enough that the ring holds 4-6 stages (the
-  // copies of a stage take longer than its MMAs)
-  static constexpr int KC = MT <= 2 ? 16 : 8;
-  static constexpr int KP = ((K + KC - 1) / KC) * KC; // padded K
+  static constexpr int NPAD = (K + 15) / 16 * 16;     // operator rows = MMA N (<= 2 MMAs)
+  static constexpr int KC = 16;                       // K chunk per ring stage
+  static constexpr int KP = ((K + KC - 1) / KC) * KC; // padded K (== NPAD)
   static constexpr int NKC = KP / KC;
-  // TMEM accumulators: two (double-buffered epilogue) when they fit in the
-  // 512 columns, else one
-  static constexpr int TBUF = 2 * MT * 128 <= 512 ? 2 : 1;
-  static constexpr int TMEM_COLS = TBUF * MT * 128 <= 256 ? 256 : 512;
-  // one stage: A hi/lo (MP x KC) + B hi/lo (128 x KC) floats
-  static constexpr int STAGE_FLOATS = 2 * MP * KC + 2 * kNTile * KC;
-  // stages of the copy ring: as many as ~220 KB of shared memory holds (at
-  // most 6), and at most NKC + 1, so the copies run at most one tile ahead
-  static constexpr int NS_SMEM = (220 * 1024) / (STAGE_FLOATS * (int)sizeof(float));
+  // TMEM accumulators of 128 lanes x NPAD columns: two (double-buffered
+  // epilogue) at a 256-column stride when they fit in the 512 columns
+  static constexpr int BSTRIDE = NPAD <= 128 ? 128 : 256;
+  static constexpr int TBUF = NPAD <= 256 ? 2 : 1;
+  static constexpr int TMEM_COLS = TBUF * BSTRIDE <= 256 && NPAD <= 256 ? 256 : 512;
+  // one stage: multipole rows hi/lo (128 x KC) + operator rows hi/lo (NPAD x KC)
+  static constexpr int STAGE_FLOATS = 2 * kNTile * KC + 2 * NPAD * KC;
+  // the epilogue's transpose buffers: per epilogue warp 32 pairs x 32 outputs
+  // at a row stride of 36 floats (conflict-free 16-byte accesses)
+  static constexpr int EPI_STRIDE = 36;
+  static constexpr int EPI_FLOATS = 8 * 32 * EPI_STRIDE;
+  // stages of the copy ring: as many as the rest of ~220 KB of shared memory
+  // holds (at most 6), and at most NKC + 1, so the copies run at most one
+  // tile ahead
+  static constexpr int NS_SMEM =
+      (220 * 1024 - EPI_FLOATS * (int)sizeof(float)) / (STAGE_FLOATS * (int)sizeof(float));
   static constexpr int NS_CAP = NS_SMEM < 6 ? NS_SMEM : 6;
   static constexpr int NS = NS_CAP < NKC + 1 ? NS_CAP : NKC + 1;
   static_assert(NS >= 2, "the copy ring needs two stages");
-  static constexpr size_t SMEM = (size_t)NS * STAGE_FLOATS * sizeof(float) + 1024;
-  // An output row of degree j reads only sources of degree n < P - j, so
-  // M-tile mt (rows of degree >= jmin(mt)) has nonzero operator entries in
-  // its first kc_need(mt) K-chunks only; chunk kc is read by the first
-  // mcount(kc) M-tiles (kc_need falls with mt).
-  static constexpr int jmin(int mt) {
-    int j = 0;
-    while ((j + 1) * (j + 2) / 2 <= 64 * mt) j++;
-    return j;
+  static constexpr size_t SMEM = ((size_t)NS * STAGE_FLOATS + EPI_FLOATS) * sizeof(float) + 1024;
+  // Chunk kc holds source coefficients 8 kc .. 8 kc + 7, of degree >= nmin;
+  // the outputs of degree j < P - nmin, the first (P - nmin)(P - nmin + 1)
+  // real rows, are the ones it reaches (rounded up to the MMA's N step).
+  static constexpr int nmin(int kc) {
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= (KC / 2) * kc) n++;
+    return n;
   }
-  static constexpr int kc_need(int mt) {
-    if (kDense) return NKC;
-    const int c = ((P - jmin(mt)) * (P - jmin(mt) + 1) + KC - 1) / KC;
-    return c < NKC ? c : NKC;
-  }
-  static constexpr int mcount(int kc) {
-    int m = 0;
-    for (int mt = 0; mt < MT; mt++) m += kc_need(mt) > kc ? 1 : 0;
-    return m;
+  static constexpr int nrows(int kc) {
+    if (kDense) return NPAD;
+    const int r = ((P - nmin(kc)) * (P - nmin(kc) + 1) + 15) / 16 * 16;
+    return r < NPAD ? r : NPAD;
   }
 };
 
@@ -337,7 +340,7 @@ __device__ __forceinline__ float tf32_round(float x) {
 template <int P>
 __device__ __forceinline__ size_t op_offset(int r, int c) {
   using S = TcShape<P>;
-  return ((size_t)(c / S::KC) * (S::MP / 8) + (size_t)(r / 8)) * (S::KC / 4 * 32) +
+  return ((size_t)(c / S::KC) * (S::NPAD / 8) + (size_t)(r / 8)) * (S::KC / 4 * 32) +
          (size_t)((c % S::KC) / 4) * 32 + (size_t)(r % 8) * 4 + (size_t)(c % 4);
 }
 
@@ -371,10 +374,10 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *hi = ops_hi + (size_t)cls * S::MP * S::KP;
-  float *lo = ops_lo + (size_t)cls * S::MP * S::KP;
+  float *hi = ops_hi + (size_t)cls * S::NPAD * S::KP;
+  float *lo = ops_lo + (size_t)cls * S::NPAD * S::KP;
   // one thread per complex (output, input) pair: its real 2 x 2 block
-  for (int idx = threadIdx.x; idx < (S::MP / 2) * (S::KP / 2); idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // complex output / input
     double v00 = 0, v01 = 0, v10 = 0, v11 = 0;  // [row re/im][column re/im]
     if (2 * to < S::K && 2 * ti < S::K) {
@@ -414,14 +417,14 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
 }
 
 // Per cell c (one warp each): Mt[c][2t + (0: re, 1: im)] = M[c][t] / w^n
-// (n = degree of t, w = the cell's width), split into TF32 hi + lo.
+// (n = degree of t, w = the cell's width) in FP32; the GEMM splits each row
+// into TF32 hi + lo as it stages it.
 template <int P>
 __global__ void __launch_bounds__(256) normalize_M(int64_t ncells, const int32_t *__restrict__ cnb,
                                                    const double *__restrict__ cmin,
                                                    const double *__restrict__ cmax,
                                                    const double2 *__restrict__ M,
-                                                   float *__restrict__ Mt_hi,
-                                                   float *__restrict__ Mt_lo) {
+                                                   float *__restrict__ Mt) {
   using S = TcShape<P>;
   constexpr int kSlots = (S::KP + 31) / 32;
   __shared__ double pw[8][P];  // per warp: w^-n
@@ -449,9 +452,7 @@ __global__ void __launch_bounds__(256) normalize_M(int64_t ncells, const int32_t
         const double2 z = M[c * S::NT + (kk >> 1)];
         v = (float)(((kk & 1) ? z.y : z.x) * pw[wi][deg[r]]);
       }
-      const float h = tf32_round(v);
-      Mt_hi[c * S::KP + kk] = h;
-      Mt_lo[c * S::KP + kk] = tf32_round(v - h);
+      Mt[c * S::KP + kk] = v;
     }
   }
 }
@@ -581,15 +582,16 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t 
                "r"(src_bytes)
                : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
 // Arrive on `bar` once all of this thread's earlier cp.async copies have landed
 // (the barrier's expected count includes this arrival).
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
+
 // Bulk copy of `bytes` (a multiple of 16) global -> shared, completing on `bar`.
 __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes,
                                           uint64_t *bar) {
@@ -623,33 +625,35 @@ __device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volat
   return true;
 }
 
-// MMAs of one k-chunk: for each M-tile, KC/8 k-steps of three tf32 MMAs
-// (hi*hi, lo*hi, hi*lo) into TMEM columns dcol + [mt*128, mt*128+128).
-// a_hi/a_lo point at the chunk's operator rows (core-matrix layout), b_hi/b_lo
-// at the chunk's 128 multipole rows.
+// MMAs of one k-chunk: KC/8 k-steps of three tf32 MMAs (hi*hi, lo*hi,
+// hi*lo) of the 128 multipole rows (A) against the operator rows the chunk
+// reaches (B, N = nrows(kc), as two MMAs where that exceeds 256) into TMEM
+// columns dcol + [0, N).  a_*: the chunk's multipole rows, b_*: its operator
+// rows, both K-major core matrices.
 template <int P, bool kDense = false>
 __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, uint32_t a_lo,
                                                  uint32_t b_hi, uint32_t b_lo, int kc) {
   using S = TcShape<P, kDense>;
-  const int mcnt = S::mcount(kc);  // M-tiles with nonzero operator entries in this chunk
-  // instruction descriptor: D f32, A/B tf32, K-major both, N = 128, M = 128
-  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
-                         ((uint32_t)(128 >> 4) << 24);
+  const int nr = S::nrows(kc);
   const uint32_t LBO = 128;                  // adjacent k-cores
   const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
 #pragma unroll
-  for (int mt = 0; mt < S::MT; mt++) {
-    if (mt >= mcnt) break;
-    const uint32_t aoff = (uint32_t)mt * 16u * SBO;  // 16 row groups per M-tile
-    const uint32_t d = dcol + (uint32_t)(mt * kNTile);
+  for (int s = 0; s < S::KC / 8; s++) {
+    const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
+    const uint64_t ah = umma_desc(a_hi + koff, LBO, SBO);
+    const uint64_t al = umma_desc(a_lo + koff, LBO, SBO);
+    const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
 #pragma unroll
-    for (int s = 0; s < S::KC / 8; s++) {
-      const uint32_t koff = (uint32_t)s * 256u;  // two k-cores
-      const uint64_t ah = umma_desc(a_hi + aoff + koff, LBO, SBO);
-      const uint64_t al = umma_desc(a_lo + aoff + koff, LBO, SBO);
-      const uint64_t bh = umma_desc(b_hi + koff, LBO, SBO);
-      const uint64_t bl = umma_desc(b_lo + koff, LBO, SBO);
-      const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
+    for (int n0 = 0; n0 < S::NPAD; n0 += 256) {
+      if (n0 >= nr) break;
+      const int nn = nr - n0 < 256 ? nr - n0 : 256;
+      // instruction descriptor: D f32, A/B tf32, K-major both, N = nn, M = 128
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(nn >> 3) << 17) |
+                             ((uint32_t)(128 >> 4) << 24);
+      const uint32_t boff = (uint32_t)(n0 / 8) * SBO + koff;
+      const uint64_t bh = umma_desc(b_hi + boff, LBO, SBO);
+      const uint64_t bl = umma_desc(b_lo + boff, LBO, SBO);
+      const uint32_t d = dcol + (uint32_t)n0;
       umma_tf32(d, ah, bh, idesc, acc);
       umma_tf32(d, al, bh, idesc, 1u);
       umma_tf32(d, ah, bl, idesc, 1u);
@@ -657,37 +661,49 @@ __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, u
   }
 }
 
+__device__ __forceinline__ void red_add_v4(float *p, uint32_t a, uint32_t b, uint32_t c,
+                                           uint32_t d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(__uint_as_float(a)),
+               "f"(__uint_as_float(b)), "f"(__uint_as_float(c)), "f"(__uint_as_float(d))
+               : "memory");
+}
+
 // Warp roles of the GEMM kernel.
 constexpr int kProdThreads = 256;  // warps 0-7: copies into the stage ring
 constexpr int kEpiWarp0 = 8;       // warps 8-15: epilogue (TMEM lane quarter warp % 4,
 constexpr int kEpiWarps = 8;       //   column half (warp - 8) / 4)
 constexpr int kMmaWarp = 16;       // warp 16: TMEM allocation, MMA issue (lane 0)
-constexpr int kThreadsTc = 32 * 17;
+constexpr int kSplitWarp0 = 17;    // warps 17-24: split the staged rows into hi + lo
+constexpr int kSplitThreads = 256;
+constexpr int kThreadsTc = 32 * 25;
 
 // Persistent CTA over the tiles blockIdx.x, blockIdx.x + gridDim.x, ...,
 // warp-specialised; the roles meet only at mbarriers:
 //  - producers (warps 0-7) walk the (tile, k-chunk) steps through an NS-stage
-//    ring: thread 0 bulk-copies the step's operator chunk (A, contiguous, hi
-//    and lo); every producer cp.async-copies its share of the 128 gathered
-//    multipole rows (B, pre-split hi/lo; lanes of a warp cover whole row
-//    segments) and arrives on full[stage] once they
-//    have landed.  A stage is refilled after the MMAs that read it commit to
-//    empty[stage].
+//    ring: every producer cp.async-copies its share of the 128 gathered
+//    multipole rows (A, FP32; lanes of a warp cover whole row segments) and
+//    arrives on landed[stage] when they have landed; thread 0 bulk-copies
+//    the operator rows the chunk reaches (B, contiguous, hi and lo), which
+//    complete on full[stage].  A stage is refilled after the MMAs that read
+//    it commit to empty[stage].
+//  - the split warps (17-24) wait for landed[stage], split the rows into
+//    TF32 hi + lo in place and arrive on full[stage].
 //  - the MMA thread (warp 16, lane 0) waits for full[stage], issues the
 //    chunk's 3xTF32 MMAs into one of TBUF TMEM accumulators and commits them
 //    to empty[stage]; after a tile's last chunk it commits to tfull[buffer].
 //  - the epilogue warps (8-15) wait for tfull[buffer], read the accumulator
-//    with tcgen05.ld and add column j into row target(j) of Lt, then arrive on
-//    tempty[buffer], which the MMA thread waits for before reusing it; with
-//    two TMEM buffers the epilogue of tile i overlaps the MMAs of tile i+1.
+//    with tcgen05.ld (TMEM lane = pair, column = output) and add each pair's
+//    outputs into its target's Lt row, then arrive on tempty[buffer], which
+//    the MMA thread waits for before reusing it; with two TMEM buffers the
+//    epilogue of tile i overlaps the MMAs of tile i+1.
 // Every wait is bounded and also gives up when another role has aborted; the
 // CTA then drains its copies and its MMAs before freeing TMEM.
 template <int P, bool kDense = false>
 __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
     const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
-    const float *__restrict__ ops_lo, const float *__restrict__ Mt_hi,
-    const float *__restrict__ Mt_lo, float *__restrict__ Lt, int *__restrict__ err,
+    const float *__restrict__ ops_lo, const float *__restrict__ Mt, float *__restrict__ Lt,
+    int *__restrict__ err,
     long long wait_limit) {
   using S = TcShape<P, kDense>;
   constexpr int NS = S::NS;
@@ -695,7 +711,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   float *base = reinterpret_cast<float *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full[NS], empty[NS], tfull[2], tempty[2], fin;
+  __shared__ __align__(8) uint64_t landed[NS], full[NS], empty[NS], tfull[2], tempty[2], fin;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
   volatile int *abort = &abort_sh;
@@ -704,7 +720,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
   const uint64_t mask = (1ull << shift) - 1;
   if (tid == 0) {
     for (int i = 0; i < NS; i++) {
-      mbar_init(&full[i], kProdThreads + 1);
+      mbar_init(&landed[i], kProdThreads);
+      mbar_init(&full[i], kSplitThreads + 1);
       mbar_init(&empty[i], 1);
     }
     for (int b = 0; b < 2; b++) {
@@ -735,11 +752,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
 
   if (warp < kEpiWarp0) {
     // ---------------- producers ----------------
-    // B: each row chunk is KC floats = PPR 16-byte pieces.  A warp copies 8
+    // A: each row chunk is KC floats = PPR 16-byte pieces.  A warp copies 8
     // rows x PPR pieces (PPR <= 4): lane l takes row l % 8 of the warp's
     // group and piece l / 8, so its shared-memory writes fill whole core
     // matrices (8 rows x 16 bytes, no bank conflicts) and each row's chunk is
-    // read as PPR x 16 contiguous bytes.  Thread t copies rows brow0 + i * RPP
+    // read as PPR x 16 contiguous bytes.  Thread t copies rows arow0 + i * RPP
     // (RPP = rows per pass of all producers, i < NRT) and fetches their
     // sources and the tile's class one tile ahead.
     constexpr int PPR = S::KC / 4;
@@ -747,7 +764,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     constexpr int RPW = 32 / PPR;  // rows per warp instruction
     constexpr int RPP = (kProdThreads / 32) * RPW;
     constexpr int NRT = kNTile / RPP;
-    const int bpiece = (tid & 31) / RPW, brow0 = (tid >> 5) * RPW + (tid & 31) % RPW;
+    const int apiece = (tid & 31) / RPW, arow0 = (tid >> 5) * RPW + (tid & 31) % RPW;
     int cur_src[NRT], nxt_src[NRT];
     int cur_cls = 0, nxt_cls = 0;
     auto fetch = [&](int64_t jt) {
@@ -761,7 +778,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       }
 #pragma unroll
       for (int i = 0; i < NRT; i++) {
-        const int row = brow0 + i * RPP;
+        const int row = arow0 + i * RPP;
         nxt_src[i] = row < it.len ? (int)(list[sorted_vals[it.start + row]] & mask) : -1;
       }
     };
@@ -769,7 +786,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     int64_t issued = 0;
     for (int64_t step = 0; step < nsteps; step++) {
       const int st = (int)(step % NS);
-      if (step >= NS && !wait_phase(&empty[st], (uint32_t)((step / NS - 1) & 1), abort, wait_limit)) break;
+      if (step >= NS &&
+          !wait_phase(&empty[st], (uint32_t)((step / NS - 1) & 1), abort, wait_limit))
+        break;
       const int64_t jt = step / S::NKC;
       const int kc = (int)(step % S::NKC);
       if (kc == 0) {
@@ -778,28 +797,26 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
         cur_cls = nxt_cls;
       }
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
-      float *sA_lo = sA_hi + S::MP * S::KC;
-      float *sB_hi = sA_lo + S::MP * S::KC;
-      float *sB_lo = sB_hi + kNTile * S::KC;
+      float *sB_hi = sA_hi + 2 * kNTile * S::KC;
+      float *sB_lo = sB_hi + S::NPAD * S::KC;
       if (tid == 0) {
-        const size_t aoff = (size_t)cur_cls * S::MP * S::KP + (size_t)kc * S::MP * S::KC;
-        // the chunk's rows of the M-tiles that read it: a prefix of its block
-        const uint32_t abytes = (uint32_t)(S::mcount(kc) * 128 * S::KC * sizeof(float));
-        mbar_expect_tx(&full[st], 2 * abytes);
-        bulk_copy(sA_hi, ops_hi + aoff, abytes, &full[st]);
-        bulk_copy(sA_lo, ops_lo + aoff, abytes, &full[st]);
+        const size_t boff = (size_t)cur_cls * S::NPAD * S::KP + (size_t)kc * S::NPAD * S::KC;
+        // the chunk's operator rows that it reaches: a prefix of its block
+        const uint32_t bbytes = (uint32_t)(S::nrows(kc) * S::KC * sizeof(float));
+        mbar_expect_tx(&full[st], 2 * bbytes);
+        bulk_copy(sB_hi, ops_hi + boff, bbytes, &full[st]);
+        bulk_copy(sB_lo, ops_lo + boff, bbytes, &full[st]);
       }
 #pragma unroll
       for (int i = 0; i < NRT; i++) {
-        const int row = brow0 + i * RPP;
+        const int row = arow0 + i * RPP;
         const bool have = cur_src[i] >= 0;
-        const size_t boff = (size_t)(have ? cur_src[i] : 0) * S::KP + (size_t)kc * S::KC +
-                            4 * bpiece;
-        const int o = ((row >> 3) * PPR + bpiece) * 32 + (row & 7) * 4;
-        cp_async16(sB_hi + o, Mt_hi + boff, have ? 16u : 0u);
-        cp_async16(sB_lo + o, Mt_lo + boff, have ? 16u : 0u);
+        const size_t aoff = (size_t)(have ? cur_src[i] : 0) * S::KP + (size_t)kc * S::KC +
+                            4 * apiece;
+        const int o = ((row >> 3) * PPR + apiece) * 32 + (row & 7) * 4;
+        cp_async16(sA_hi + o, Mt + aoff, have ? 16u : 0u);
       }
-      cp_async_arrive_noinc(&full[st]);
+      cp_async_arrive_noinc(&landed[st]);
       issued = step + 1;
       // the next tile's sources (a chain of dependent loads), after this
       // tile's first copies are on their way
@@ -823,7 +840,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
         const int64_t use_b = NB == 2 ? (jt >> 1) : jt;
         if (use_b >= 1 && !wait_phase(&tempty[b], (uint32_t)((use_b - 1) & 1), abort, wait_limit)) break;
         tc_fence_after();
-        const uint32_t dcol = tmem + (uint32_t)(b * S::MT * kNTile);
+        const uint32_t dcol = tmem + (uint32_t)(b * S::BSTRIDE);
         bool ok = true;
         for (int kc = 0; kc < S::NKC; kc++) {
           const int64_t step = jt * S::NKC + kc;
@@ -835,11 +852,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
           fence_async_smem();  // the cp.async rows are visible to the tensor core
           tc_fence_after();
           float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
-          float *sA_lo = sA_hi + S::MP * S::KC;
-          float *sB_hi = sA_lo + S::MP * S::KC;
-          float *sB_lo = sB_hi + kNTile * S::KC;
+          float *sA_lo = sA_hi + kNTile * S::KC;
+          float *sB_hi = sA_lo + kNTile * S::KC;
+          float *sB_lo = sB_hi + S::NPAD * S::KC;
           issue_chunk_mmas<P, kDense>(dcol, smem_u32(sA_hi), smem_u32(sA_lo), smem_u32(sB_hi),
-                              smem_u32(sB_lo), kc);
+                                      smem_u32(sB_lo), kc);
           umma_commit(&empty[st]);
         }
         if (!ok) break;
@@ -852,46 +869,79 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       }
     }
     __syncwarp();
+  } else if (warp >= kSplitWarp0) {
+    // ---------------- split ----------------
+    // once a stage's FP32 rows have landed, each thread splits 8 of its 2048
+    // values into TF32 hi + lo in place, then arrives on full[stage]
+    const int t = tid - kSplitWarp0 * 32;
+    for (int64_t step = 0; step < nsteps; step++) {
+      const int st = (int)(step % NS);
+      if (!wait_phase(&landed[st], (uint32_t)((step / NS) & 1), abort, wait_limit)) break;
+      float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
+      float *sA_lo = sA_hi + kNTile * S::KC;
+#pragma unroll
+      for (int i = 0; i < (kNTile * S::KC) / (4 * kSplitThreads); i++) {
+        const int o = 4 * (t + i * kSplitThreads);
+        const float4 x = *reinterpret_cast<const float4 *>(sA_hi + o);
+        float4 hi, lo;
+        hi.x = tf32_round(x.x); lo.x = tf32_round(x.x - hi.x);
+        hi.y = tf32_round(x.y); lo.y = tf32_round(x.y - hi.y);
+        hi.z = tf32_round(x.z); lo.z = tf32_round(x.z - hi.z);
+        hi.w = tf32_round(x.w); lo.w = tf32_round(x.w - hi.w);
+        *reinterpret_cast<float4 *>(sA_hi + o) = hi;
+        *reinterpret_cast<float4 *>(sA_lo + o) = lo;
+      }
+      fence_async_smem();  // the split rows are visible to the tensor core
+      mbar_arrive(&full[st]);
+    }
   } else {
     // ---------------- epilogue ----------------
-    const int q = warp & 3;                   // TMEM lane quarter of this warp (warp % 4)
-    const int h = (warp - kEpiWarp0) >> 2;    // column half
-    int tg[2], tg_next[2];   // targets of columns 64h + 32c + lane, this tile and the next
-    auto load_targets = [&](int64_t jt, int (&t)[2]) {
+    // warp (q, h): TMEM lanes 32 q .. 32 q + 31 (pairs of the tile), column
+    // groups of 32 outputs g = h, h + 2, ...  Each 32 x 32 block goes through
+    // the warp's shared-memory buffer so that one reduction instruction adds
+    // 4 pairs x 32 consecutive outputs (4 rows of Lt, 128 bytes each).
+    const int q = warp & 3;
+    const int h = (warp - kEpiWarp0) >> 2;
+    constexpr int NG = (S::NPAD + 31) / 32;
+    float *xb = base + (size_t)NS * S::STAGE_FLOATS + (warp - kEpiWarp0) * 32 * S::EPI_STRIDE;
+    int tg = -1, tg_next = -1;  // target of this lane's pair, this tile and the next
+    auto load_target = [&](int64_t jt) {
       TileItem it;
       it.len = 0;
       it.start = 0;
       if (jt < ntiles) it = item_of(jt);
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        const int col = h * 64 + c * 32 + lane;
-        t[c] = col < it.len ? (int)(list[sorted_vals[it.start + col]] >> shift) : -1;
-      }
+      const int p = q * 32 + lane;
+      return p < it.len ? (int)(list[sorted_vals[it.start + p]] >> shift) : -1;
     };
-    load_targets(0, tg_next);
+    tg_next = load_target(0);
     for (int64_t jt = 0; jt < ntiles; jt++) {
       const int b = NB == 2 ? (int)(jt & 1) : 0;
       const int64_t use_b = NB == 2 ? (jt >> 1) : jt;
-#pragma unroll
-      for (int c = 0; c < 2; c++) tg[c] = tg_next[c];
-      load_targets(jt + 1, tg_next);
+      tg = tg_next;
+      tg_next = load_target(jt + 1);
       if (!wait_phase(&tfull[b], (uint32_t)(use_b & 1), abort, wait_limit)) break;
       tc_fence_after();
 #pragma unroll 1
-      for (int mt = 0; mt < S::MT; mt++) {
-        const int r = mt * 128 + q * 32 + lane;
+      for (int g = h; g < NG; g += 2) {
+        uint32_t v[32];
+        const uint32_t taddr =
+            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * S::BSTRIDE + g * 32);
+        tmem_ld32(taddr, v);
 #pragma unroll
-        for (int c = 0; c < 2; c++) {
-          uint32_t v[32];
-          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
-                                 (uint32_t)(b * S::MT * kNTile + mt * kNTile + h * 64 + c * 32);
-          tmem_ld32(taddr, v);
+        for (int c = 0; c < 32; c += 4)
+          *reinterpret_cast<uint4 *>(xb + lane * S::EPI_STRIDE + c) =
+              make_uint4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+        __syncwarp();
+        const int c4 = 4 * (lane & 7);
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int t = __shfl_sync(0xffffffffu, tg[c], j);
-            if (t >= 0 && r < S::K) atomicAdd(Lt + (size_t)t * S::KP + r, __uint_as_float(v[j]));
-          }
+        for (int k = 0; k < 8; k++) {
+          const int pr = 4 * k + (lane >> 3);
+          const int t = __shfl_sync(0xffffffffu, tg, pr);
+          const uint4 w = *reinterpret_cast<const uint4 *>(xb + pr * S::EPI_STRIDE + c4);
+          if (t >= 0 && g * 32 + c4 < S::NPAD)
+            red_add_v4(Lt + (size_t)t * S::KP + g * 32 + c4, w.x, w.y, w.z, w.w);
         }
+        __syncwarp();
       }
       tc_fence_before();
       __syncwarp();
@@ -1085,7 +1135,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   std::optional<PhaseTimer> setup_timer;
   setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
   M2LClassInfo ci;
-  TB_TRY(m2l_classes(ctx, 2 * sizeof(float) * (size_t)S::MP * S::KP, ci));
+  TB_TRY(m2l_classes(ctx, 2 * sizeof(float) * (size_t)S::NPAD * S::KP, ci));
   if (n == 0) {  // no M2L pair: every local expansion is zero
     TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
     TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
@@ -1093,7 +1143,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   }
   const int64_t ntc = ci.ntc, nitems = ci.nitems, n64 = ci.n64;
   int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
-  const size_t opsz = (size_t)S::MP * S::KP;
+  const size_t opsz = (size_t)S::NPAD * S::KP;
   if (ntc > 0) {
     TB_CUDA(ctx, T.ops_hi.ensure(opsz * ntc, s));
     TB_CUDA(ctx, T.ops_lo.ensure(opsz * ntc, s));
@@ -1101,11 +1151,11 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
     TB_LAUNCH_CHECK(ctx);
   }
   // 4. normalised multipoles, zeroed normalised locals
-  TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));  // hi rows, then lo rows
+  TB_CUDA(ctx, T.Mt.ensure((size_t)C * S::KP, s));
   TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
   if (!T.mt_ready) {  // the mixed upward pass leaves them ready
     normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
-        C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p, T.Mt.p + (size_t)C * S::KP);
+        C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, T.Mt.p);
     TB_LAUNCH_CHECK(ctx);
   }
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
@@ -1114,7 +1164,6 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   TB_TRY(m2l_fp64_pairs(ctx, T.pairs64.p, n64));
   if (nitems > 0) {
     PhaseTimer t(ctx, &ctx->timings.m2l_tc);
-    const float *mt_hi = T.Mt.p, *mt_lo = T.Mt.p + (size_t)C * S::KP;
     const TileItem *it = reinterpret_cast<const TileItem *>(T.items.p);
     const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
     static_assert(S::SMEM <= 227 * 1024 - 4096, "shared memory");
@@ -1122,7 +1171,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(it, nitems, T.vals.p, ctx->m2l.p,
                                                         ctx->list_shift, T.ops_hi.p, T.ops_lo.p,
-                                                        mt_hi, mt_lo, T.Lt.p, T.err.p,
+                                                        T.Mt.p, T.Lt.p, T.err.p,
                                                         ctx->tc_wait_limit);
     TB_LAUNCH_CHECK(ctx);
   }
@@ -1192,9 +1241,9 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *hi = ops_hi + (size_t)o * S::MP * S::KP;
-  float *lo = ops_lo + (size_t)o * S::MP * S::KP;
-  for (int idx = threadIdx.x; idx < (S::MP / 2) * (S::KP / 2); idx += blockDim.x) {
+  float *hi = ops_hi + (size_t)o * S::NPAD * S::KP;
+  float *lo = ops_lo + (size_t)o * S::NPAD * S::KP;
+  for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // target / source coefficient
     cd a{0, 0}, b{0, 0};  // target += a * source + b * conj(source)
     if (2 * to < S::K && 2 * ti < S::K) {
@@ -1245,15 +1294,14 @@ __global__ void iota_u32(uint32_t *__restrict__ v, int64_t n) {
 }
 
 // After a level's M2M: per parent (one warp each) its normalised FP32 sum A
-// becomes the GEMM's split input row and its FP64 multipoles (A w^n).
+// becomes the next GEMM's input row and its FP64 multipoles (A w^n).
 template <int P>
 __global__ void __launch_bounds__(256) finish_parents(int64_t c0, int64_t np,
                                                       const int32_t *__restrict__ cparent,
                                                       const double *__restrict__ cmin,
                                                       const double *__restrict__ cmax,
                                                       const float *__restrict__ acc,
-                                                      float *__restrict__ Mt_hi,
-                                                      float *__restrict__ Mt_lo,
+                                                      float *__restrict__ Mt,
                                                       double2 *__restrict__ M) {
   using S = TcShape<P>;
   __shared__ double pw[8][P];
@@ -1264,12 +1312,7 @@ __global__ void __launch_bounds__(256) finish_parents(int64_t c0, int64_t np,
     __syncwarp();
     if (lane < P) pw[wi][lane] = pow(cmax[3 * p] - cmin[3 * p], lane);
     __syncwarp();
-    for (int kk = lane; kk < S::KP; kk += 32) {
-      const float v = acc[p * S::KP + kk];
-      const float h = tf32_round(v);
-      Mt_hi[p * S::KP + kk] = h;
-      Mt_lo[p * S::KP + kk] = tf32_round(v - h);
-    }
+    for (int kk = lane; kk < S::KP; kk += 32) Mt[p * S::KP + kk] = acc[p * S::KP + kk];
     for (int t = lane; t < S::NT; t += 32) {
       int j, k;
       jk_of(t, j, k);
@@ -1282,8 +1325,8 @@ __global__ void __launch_bounds__(256) finish_parents(int64_t c0, int64_t np,
 // One level's M2M GEMM: the children's split rows translated into the parents'
 // normalised rows of out (FP32, accumulated).
 template <int P>
-int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *B_hi,
-                    const float *B_lo, float *out) {
+int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *rows,
+                    float *out) {
   using S = TcShape<P, true>;
   cudaStream_t s = ctx->stream;
   auto &T = ctx->tc;
@@ -1313,7 +1356,7 @@ int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *B_
   const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
   m2l_tc_kernel<P, true><<<grid, kThreadsTc, S::SMEM, s>>>(
       reinterpret_cast<const TileItem *>(T.tree_items.p), nitems, T.iota.p, T.tree_list.p,
-      kTreeShift, T.ops_tr_hi.p, T.ops_tr_lo.p, B_hi, B_lo, out, T.err.p, ctx->tc_wait_limit);
+      kTreeShift, T.ops_tr_hi.p, T.ops_tr_lo.p, rows, out, T.err.p, ctx->tc_wait_limit);
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
 }
@@ -1348,7 +1391,7 @@ int tc_tree_prepare(tapas_b200_ctx *ctx) {
     T.iota_n = C;
   }
   if (T.tr_P != P) {
-    const size_t opsz = (size_t)S::MP * S::KP * 8;
+    const size_t opsz = (size_t)S::NPAD * S::KP * 8;
     TB_CUDA(ctx, T.ops_tr_hi.ensure(opsz, s));
     TB_CUDA(ctx, T.ops_tr_lo.ensure(opsz, s));
     build_tree_ops<P><<<8, 256, 0, s>>>(ctx->cparent.p, ctx->ccen.p, ctx->cmin.p,
@@ -1383,11 +1426,11 @@ int tc_tree_upward_P(tapas_b200_ctx *ctx) {
   cudaStream_t s = ctx->stream;
   const int64_t C = ctx->ncells;
   auto &T = ctx->tc;
-  TB_CUDA(ctx, T.Mt.ensure(2 * (size_t)C * S::KP, s));
+  TB_CUDA(ctx, T.Mt.ensure((size_t)C * S::KP, s));
   TB_CUDA(ctx, T.Lt.ensure((size_t)C * S::KP, s));
-  float *mt_hi = T.Mt.p, *mt_lo = T.Mt.p + (size_t)C * S::KP;
+  float *mt = T.Mt.p;
   normalize_M<P><<<grid_for(C, 8, ctx->num_sms * 8), 256, 0, s>>>(
-      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt_hi, mt_lo);
+      C, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt);
   TB_LAUNCH_CHECK(ctx);
   const int nlev = tree_parent_levels(ctx), l0 = first_tc_tree_level(nlev);
   if (nlev > l0) {
@@ -1396,9 +1439,9 @@ int tc_tree_upward_P(tapas_b200_ctx *ctx) {
     for (int l = nlev - 1; l >= l0; l--) {
       const int64_t c0 = ctx->level_off[l + 1], np = (ctx->level_off[l + 2] - c0) / 8;
       if (np <= 0) continue;
-      TB_TRY(tree_level_gemm<P>(ctx, c0, np, mt_hi, mt_lo, T.Lt.p));
+      TB_TRY(tree_level_gemm<P>(ctx, c0, np, mt, T.Lt.p));
       finish_parents<P><<<grid_for(np, 8, ctx->num_sms * 8), 256, 0, s>>>(
-          c0, np, ctx->cparent.p, ctx->cmin.p, ctx->cmax.p, T.Lt.p, mt_hi, mt_lo, ctx->M.p);
+          c0, np, ctx->cparent.p, ctx->cmin.p, ctx->cmax.p, T.Lt.p, mt, ctx->M.p);
       TB_LAUNCH_CHECK(ctx);
     }
     TB_TRY(check_tc_abort(ctx, "M2M"));
@@ -1409,7 +1452,7 @@ int tc_tree_upward_P(tapas_b200_ctx *ctx) {
       std::min<int64_t>(C, ctx->level_off[std::min<size_t>(l0, ctx->level_off.size() - 1)]);
   if (ctop > 0) {
     normalize_M<P><<<grid_for(ctop, 8, ctx->num_sms * 8), 256, 0, s>>>(
-        ctop, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt_hi, mt_lo);
+        ctop, ctx->cnb.p, ctx->cmin.p, ctx->cmax.p, ctx->M.p, mt);
     TB_LAUNCH_CHECK(ctx);
   }
   T.mt_ready = true;
