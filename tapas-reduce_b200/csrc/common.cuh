@@ -109,13 +109,13 @@ struct TcState {
   DBuf<int32_t> flag, scan, seg_start, tcflag, tcid, ntiles, tile_off;
   DBuf<int4> items;
   DBuf<int2> cls_range;    // per selected class: first sorted pair, pair count
-  DBuf<float> ops_hi, ops_lo, Mt, Lt;
+  DBuf<float> ops, Mt, Lt;  // per selected class its FP32 operator rows; FP32 rows of M, L
   DBuf<double> ops64, Mt64, Lt64;  // FP64 class GEMM (plain form)
   DBuf<uint8_t> use64;     // FP64 class GEMM: list entries left to the pair kernel
   DBuf<int32_t> oflag, opos;  // sharded: owned sorted pairs and their compacted positions
   DBuf<uint8_t> sel, sel2;    // sharded: class selection per sorted / compacted pair
   // tensor-core M2M of the mixed form
-  DBuf<float> ops_tr_hi, ops_tr_lo;  // 8 M2M classes: octant o
+  DBuf<float> ops_tr;                // 8 M2M classes: octant o
   int tr_P = 0;                      // order they were built for (0: none)
   DBuf<uint64_t> tree_list;          // one level's (parent << 32 | child) pairs
   DBuf<uint32_t> iota;               // 0, 1, 2, ... (pair order of a level)
@@ -127,9 +127,9 @@ struct TcState {
     keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();
     pairs64.release(); flag.release(); scan.release(); seg_start.release(); tcflag.release();
     tcid.release(); ntiles.release(); tile_off.release(); items.release(); cls_range.release();
-    ops_hi.release(); ops_lo.release(); Mt.release(); Lt.release(); ops64.release();
+    ops.release(); Mt.release(); Lt.release(); ops64.release();
     Mt64.release(); Lt64.release(); use64.release(); oflag.release(); opos.release();
-    sel.release(); sel2.release(); ops_tr_hi.release(); ops_tr_lo.release(); tree_list.release();
+    sel.release(); sel2.release(); ops_tr.release(); tree_list.release();
     iota.release(); tree_items.release(); err.release();
     tr_P = 0;
     iota_n = 0;

@@ -94,6 +94,14 @@ struct TcShape {
     const int r = ((P - nmin(kc)) * (P - nmin(kc) + 1) + 15) / 16 * 16;
     return r < NPAD ? r : NPAD;
   }
+  // An operator is stored as its chunks' reached rows only (FP32, K-major
+  // core matrices): chunk kc at choff(kc), OPS_FLOATS per operator.
+  static constexpr int choff(int kc) {
+    int o = 0;
+    for (int k = 0; k < kc; k++) o += nrows(k) * KC;
+    return o;
+  }
+  static constexpr int OPS_FLOATS = choff(NKC);
 };
 
 // ---------------------------------------------------------------------------
@@ -337,23 +345,39 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float(r);
 }
 
-template <int P>
-__device__ __forceinline__ size_t op_offset(int r, int c) {
-  using S = TcShape<P>;
-  return ((size_t)(c / S::KC) * (S::NPAD / 8) + (size_t)(r / 8)) * (S::KC / 4 * 32) +
-         (size_t)((c % S::KC) / 4) * 32 + (size_t)(r % 8) * 4 + (size_t)(c % 4);
+// Per-chunk tables of a shape (filled by one thread): reached rows nr[kc]
+// and operator offsets co[kc] (co[NKC] = OPS_FLOATS).
+template <class S>
+__device__ __forceinline__ void chunk_tables(int *nr, int *co) {
+  int o = 0;
+  for (int kc = 0; kc < S::NKC; kc++) {
+    nr[kc] = S::nrows(kc);
+    co[kc] = o;
+    o += nr[kc] * S::KC;
+  }
+  co[S::NKC] = o;
+}
+
+// Offset of operator entry (row r, column c) within an operator; the entry
+// must lie in a row its chunk reaches (r < nr[c / KC]).
+template <class S>
+__device__ __forceinline__ int op_offset(const int *co, int r, int c) {
+  return co[c / S::KC] + (r / 8) * (S::KC / 4 * 32) + ((c % S::KC) / 4) * 32 + (r % 8) * 4 +
+         (c % 4);
 }
 
 // One block per tensor-core class: unit-offset singular harmonics (evalLocal,
-// :102-135) in FP64, then every real operator entry, split hi/lo.
+// :102-135) in FP64, then every real operator entry the GEMM reads, in FP32
+// (the GEMM splits it into TF32 hi + lo in shared memory).
 template <int P>
 __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restrict__ tc_keys,
-                                                       float *__restrict__ ops_hi,
-                                                       float *__restrict__ ops_lo) {
+                                                       float *__restrict__ ops) {
   using S = TcShape<P>;
   __shared__ cd Y[P * P];
   __shared__ double scale[P];                        // (w_s / w_t)^n = 2^(delta n)
   __shared__ unsigned char deg[S::NT], ord[S::NT];   // (j, k) of coefficient t
+  __shared__ int nr[S::NKC], co[S::NKC + 1];
+  if (threadIdx.x == 0) chunk_tables<S>(nr, co);
   const int cls = blockIdx.x;
   const uint64_t key = tc_keys[cls];
   const int delta = (int)((key >> 42) & 63) - 32;
@@ -374,11 +398,11 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *hi = ops_hi + (size_t)cls * S::NPAD * S::KP;
-  float *lo = ops_lo + (size_t)cls * S::NPAD * S::KP;
+  float *op = ops + (size_t)cls * S::OPS_FLOATS;
   // one thread per complex (output, input) pair: its real 2 x 2 block
   for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // complex output / input
+    if (2 * to >= nr[(2 * ti) / S::KC]) continue;  // a row its chunk does not reach
     double v00 = 0, v01 = 0, v10 = 0, v11 = 0;  // [row re/im][column re/im]
     if (2 * to < S::K && 2 * ti < S::K) {
       const int j = deg[to], k = ord[to], n = deg[ti], ma = ord[ti];
@@ -406,13 +430,8 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
     }
     const double v[4] = {v00, v01, v10, v11};
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float f = (float)v[e];
-      const float h = tf32_round(f);
-      const size_t o = op_offset<P>(2 * to + (e >> 1), 2 * ti + (e & 1));
-      hi[o] = h;
-      lo[o] = tf32_round(f - h);
-    }
+    for (int e = 0; e < 4; e++)
+      op[op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1))] = (float)v[e];
   }
 }
 
@@ -632,9 +651,8 @@ __device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity, volat
 // rows, both K-major core matrices.
 template <int P, bool kDense = false>
 __device__ __forceinline__ void issue_chunk_mmas(uint32_t dcol, uint32_t a_hi, uint32_t a_lo,
-                                                 uint32_t b_hi, uint32_t b_lo, int kc) {
+                                                 uint32_t b_hi, uint32_t b_lo, int kc, int nr) {
   using S = TcShape<P, kDense>;
-  const int nr = S::nrows(kc);
   const uint32_t LBO = 128;                  // adjacent k-cores
   const uint32_t SBO = (S::KC / 4) * 128;    // adjacent 8-row groups
 #pragma unroll
@@ -701,9 +719,8 @@ constexpr int kThreadsTc = 32 * 25;
 template <int P, bool kDense = false>
 __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     const TileItem *__restrict__ items, int64_t nitems, const uint32_t *__restrict__ sorted_vals,
-    const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops_hi,
-    const float *__restrict__ ops_lo, const float *__restrict__ Mt, float *__restrict__ Lt,
-    int *__restrict__ err,
+    const uint64_t *__restrict__ list, int shift, const float *__restrict__ ops,
+    const float *__restrict__ Mt, float *__restrict__ Lt, int *__restrict__ err,
     long long wait_limit) {
   using S = TcShape<P, kDense>;
   constexpr int NS = S::NS;
@@ -714,14 +731,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
   __shared__ __align__(8) uint64_t landed[NS], full[NS], empty[NS], tfull[2], tempty[2], fin;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
+  __shared__ int nr_sh[S::NKC], co_sh[S::NKC + 1];  // reached operator rows, offsets
   volatile int *abort = &abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint64_t mask = (1ull << shift) - 1;
   if (tid == 0) {
     for (int i = 0; i < NS; i++) {
-      mbar_init(&landed[i], kProdThreads);
-      mbar_init(&full[i], kSplitThreads + 1);
+      mbar_init(&landed[i], kProdThreads + 1);
+      mbar_init(&full[i], kSplitThreads);
       mbar_init(&empty[i], 1);
     }
     for (int b = 0; b < 2; b++) {
@@ -730,6 +748,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     }
     mbar_init(&fin, 1);
     abort_sh = 0;
+    chunk_tables<S>(nr_sh, co_sh);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == kMmaWarp) {
@@ -798,14 +817,12 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       }
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sB_hi = sA_hi + 2 * kNTile * S::KC;
-      float *sB_lo = sB_hi + S::NPAD * S::KC;
       if (tid == 0) {
-        const size_t boff = (size_t)cur_cls * S::NPAD * S::KP + (size_t)kc * S::NPAD * S::KC;
-        // the chunk's operator rows that it reaches: a prefix of its block
-        const uint32_t bbytes = (uint32_t)(S::nrows(kc) * S::KC * sizeof(float));
-        mbar_expect_tx(&full[st], 2 * bbytes);
-        bulk_copy(sB_hi, ops_hi + boff, bbytes, &full[st]);
-        bulk_copy(sB_lo, ops_lo + boff, bbytes, &full[st]);
+        // the chunk's operator rows (the ones it reaches), FP32, into the hi area
+        const size_t boff = (size_t)cur_cls * S::OPS_FLOATS + (size_t)co_sh[kc];
+        const uint32_t bbytes = (uint32_t)(nr_sh[kc] * S::KC * sizeof(float));
+        mbar_expect_tx(&landed[st], bbytes);
+        bulk_copy(sB_hi, ops + boff, bbytes, &landed[st]);
       }
 #pragma unroll
       for (int i = 0; i < NRT; i++) {
@@ -856,7 +873,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
           float *sB_hi = sA_lo + kNTile * S::KC;
           float *sB_lo = sB_hi + S::NPAD * S::KC;
           issue_chunk_mmas<P, kDense>(dcol, smem_u32(sA_hi), smem_u32(sA_lo), smem_u32(sB_hi),
-                                      smem_u32(sB_lo), kc);
+                                      smem_u32(sB_lo), kc, nr_sh[kc]);
           umma_commit(&empty[st]);
         }
         if (!ok) break;
@@ -871,26 +888,35 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     __syncwarp();
   } else if (warp >= kSplitWarp0) {
     // ---------------- split ----------------
-    // once a stage's FP32 rows have landed, each thread splits 8 of its 2048
-    // values into TF32 hi + lo in place, then arrives on full[stage]
+    // once a stage's FP32 multipole rows and operator rows have landed, the
+    // 256 threads split them into TF32 hi + lo in place (16 bytes at a time),
+    // then arrive on full[stage]
     const int t = tid - kSplitWarp0 * 32;
+    auto split4 = [](float *hi_p, float *lo_p) {
+      const float4 x = *reinterpret_cast<const float4 *>(hi_p);
+      float4 hi, lo;
+      hi.x = tf32_round(x.x); lo.x = tf32_round(x.x - hi.x);
+      hi.y = tf32_round(x.y); lo.y = tf32_round(x.y - hi.y);
+      hi.z = tf32_round(x.z); lo.z = tf32_round(x.z - hi.z);
+      hi.w = tf32_round(x.w); lo.w = tf32_round(x.w - hi.w);
+      *reinterpret_cast<float4 *>(hi_p) = hi;
+      *reinterpret_cast<float4 *>(lo_p) = lo;
+    };
     for (int64_t step = 0; step < nsteps; step++) {
       const int st = (int)(step % NS);
+      const int kc = (int)(step % S::NKC);
       if (!wait_phase(&landed[st], (uint32_t)((step / NS) & 1), abort, wait_limit)) break;
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sA_lo = sA_hi + kNTile * S::KC;
+      float *sB_hi = sA_lo + kNTile * S::KC;
+      float *sB_lo = sB_hi + S::NPAD * S::KC;
 #pragma unroll
       for (int i = 0; i < (kNTile * S::KC) / (4 * kSplitThreads); i++) {
         const int o = 4 * (t + i * kSplitThreads);
-        const float4 x = *reinterpret_cast<const float4 *>(sA_hi + o);
-        float4 hi, lo;
-        hi.x = tf32_round(x.x); lo.x = tf32_round(x.x - hi.x);
-        hi.y = tf32_round(x.y); lo.y = tf32_round(x.y - hi.y);
-        hi.z = tf32_round(x.z); lo.z = tf32_round(x.z - hi.z);
-        hi.w = tf32_round(x.w); lo.w = tf32_round(x.w - hi.w);
-        *reinterpret_cast<float4 *>(sA_hi + o) = hi;
-        *reinterpret_cast<float4 *>(sA_lo + o) = lo;
+        split4(sA_hi + o, sA_lo + o);
       }
+      const int nb4 = nr_sh[kc] * S::KC / 4;
+      for (int i = t; i < nb4; i += kSplitThreads) split4(sB_hi + 4 * i, sB_lo + 4 * i);
       fence_async_smem();  // the split rows are visible to the tensor core
       mbar_arrive(&full[st]);
     }
@@ -1135,7 +1161,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   std::optional<PhaseTimer> setup_timer;
   setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
   M2LClassInfo ci;
-  TB_TRY(m2l_classes(ctx, 2 * sizeof(float) * (size_t)S::NPAD * S::KP, ci));
+  TB_TRY(m2l_classes(ctx, sizeof(float) * (size_t)S::OPS_FLOATS, ci));
   if (n == 0) {  // no M2L pair: every local expansion is zero
     TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
     TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
@@ -1143,11 +1169,9 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   }
   const int64_t ntc = ci.ntc, nitems = ci.nitems, n64 = ci.n64;
   int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
-  const size_t opsz = (size_t)S::NPAD * S::KP;
   if (ntc > 0) {
-    TB_CUDA(ctx, T.ops_hi.ensure(opsz * ntc, s));
-    TB_CUDA(ctx, T.ops_lo.ensure(opsz * ntc, s));
-    build_operators<P><<<(unsigned)ntc, 256, 0, s>>>(T.tc_keys.p, T.ops_hi.p, T.ops_lo.p);
+    TB_CUDA(ctx, T.ops.ensure((size_t)S::OPS_FLOATS * ntc, s));
+    build_operators<P><<<(unsigned)ntc, 256, 0, s>>>(T.tc_keys.p, T.ops.p);
     TB_LAUNCH_CHECK(ctx);
   }
   // 4. normalised multipoles, zeroed normalised locals
@@ -1170,8 +1194,8 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
     TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     m2l_tc_kernel<P><<<grid, kThreadsTc, S::SMEM, s>>>(it, nitems, T.vals.p, ctx->m2l.p,
-                                                        ctx->list_shift, T.ops_hi.p, T.ops_lo.p,
-                                                        T.Mt.p, T.Lt.p, T.err.p,
+                                                        ctx->list_shift, T.ops.p, T.Mt.p, T.Lt.p,
+                                                        T.err.p,
                                                         ctx->tc_wait_limit);
     TB_LAUNCH_CHECK(ctx);
   }
@@ -1213,19 +1237,19 @@ constexpr int kFp64TreeLevels = 4;
 constexpr int kTcUpLevels = 3;
 constexpr int kTreeShift = 32;  // tree pair list entries: target << 32 | source
 
-// M2M operator classes o (octant o), each split into TF32 hi + lo in the
-// GEMM's layout.  child0: the first child of any non-leaf cell; the offsets
+// M2M operator classes o (octant o), in FP32 in the dense GEMM's layout.  child0: the first child of any non-leaf cell; the offsets
 // are its octants' centre offsets in child widths (exact: +-1/2).
 template <int P>
 __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict__ cparent,
                                                       const double *__restrict__ ccen,
                                                       const double *__restrict__ cmin,
                                                       const double *__restrict__ cmax,
-                                                      int64_t child0, float *__restrict__ ops_hi,
-                                                      float *__restrict__ ops_lo) {
-  using S = TcShape<P>;
+                                                      int64_t child0, float *__restrict__ ops) {
+  using S = TcShape<P, true>;
   __shared__ cd Y[P * P];
   __shared__ unsigned char deg[S::NT], ord[S::NT];
+  __shared__ int nr[S::NKC], co[S::NKC + 1];
+  if (threadIdx.x == 0) chunk_tables<S>(nr, co);
   const int o = blockIdx.x;
   const int64_t c = child0 + o;
   const int p = cparent[c];
@@ -1241,8 +1265,7 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *hi = ops_hi + (size_t)o * S::NPAD * S::KP;
-  float *lo = ops_lo + (size_t)o * S::NPAD * S::KP;
+  float *op = ops + (size_t)o * S::OPS_FLOATS;
   for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // target / source coefficient
     cd a{0, 0}, b{0, 0};  // target += a * source + b * conj(source)
@@ -1265,13 +1288,8 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
     // [row re/im][column re/im] of the real 2 x 2 block
     const double v[4] = {a.x + b.x, b.y - a.y, a.y + b.y, a.x - b.x};
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float f = (float)v[e];
-      const float h = tf32_round(f);
-      const size_t off = op_offset<P>(2 * to + (e >> 1), 2 * ti + (e & 1));
-      hi[off] = h;
-      lo[off] = tf32_round(f - h);
-    }
+    for (int e = 0; e < 4; e++)
+      op[op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1))] = (float)v[e];
   }
 }
 
@@ -1356,7 +1374,7 @@ int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *ro
   const int grid = (int)std::min<int64_t>(nitems, ctx->num_sms);
   m2l_tc_kernel<P, true><<<grid, kThreadsTc, S::SMEM, s>>>(
       reinterpret_cast<const TileItem *>(T.tree_items.p), nitems, T.iota.p, T.tree_list.p,
-      kTreeShift, T.ops_tr_hi.p, T.ops_tr_lo.p, rows, out, T.err.p, ctx->tc_wait_limit);
+      kTreeShift, T.ops_tr.p, rows, out, T.err.p, ctx->tc_wait_limit);
   TB_LAUNCH_CHECK(ctx);
   return TAPAS_B200_OK;
 }
@@ -1391,12 +1409,9 @@ int tc_tree_prepare(tapas_b200_ctx *ctx) {
     T.iota_n = C;
   }
   if (T.tr_P != P) {
-    const size_t opsz = (size_t)S::NPAD * S::KP * 8;
-    TB_CUDA(ctx, T.ops_tr_hi.ensure(opsz, s));
-    TB_CUDA(ctx, T.ops_tr_lo.ensure(opsz, s));
-    build_tree_ops<P><<<8, 256, 0, s>>>(ctx->cparent.p, ctx->ccen.p, ctx->cmin.p,
-                                                  ctx->cmax.p, ctx->level_off[1], T.ops_tr_hi.p,
-                                                  T.ops_tr_lo.p);
+    TB_CUDA(ctx, T.ops_tr.ensure((size_t)TcShape<P, true>::OPS_FLOATS * 8, s));
+    build_tree_ops<P><<<8, 256, 0, s>>>(ctx->cparent.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
+                                        ctx->level_off[1], T.ops_tr.p);
     TB_LAUNCH_CHECK(ctx);
     T.tr_P = P;
   }
