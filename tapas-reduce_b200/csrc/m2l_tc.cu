@@ -47,7 +47,7 @@
 namespace tb {
 namespace {
 
-constexpr int kTcMin = 32;         // pairs needed for a class to use the tensor cores
+constexpr int kTcMin = 16;         // pairs needed for a class to use the tensor cores
 constexpr int kNTile = 128;        // pairs per tile (MMA N)
 constexpr int kOffBias = 8192;
 
