@@ -737,27 +737,39 @@ struct LevelGemm {
   double *part;     // split: [8][ncols][R]
 };
 
-constexpr int kGM = 64, kGN = 64, kGK = 16, kGThreads = 256;
+constexpr int kGM = 64, kGN = 64, kGK = 16, kGThreads = 256;  // class_gemm64 tiling
+constexpr int kLThreads = 128;     // level_gemm: four warps
+constexpr int kLStride = kGM + 4;  // level_gemm shared-memory row stride (doubles)
 
-// 64 x 64 output tile per block; warp w covers rows 32 (w & 1) + {2i, 2i+1,
-// 16+2i, 17+2i} (i = lane & 7) and columns 16 (w >> 1) + 4 (lane >> 3) .. +3,
-// so every shared-memory read of a warp is conflict-free.  A tiles are copied
-// as they lie (k-major); B tiles are loaded one column per lane.  The next
-// 16-source chunk is loaded into registers while the current one is
-// multiplied from shared memory (two buffers, one barrier per chunk).
-__global__ void __launch_bounds__(kGThreads, 3) level_gemm(LevelGemm g) {
-  __shared__ __align__(16) double As[2][kGK][kGM];
-  __shared__ __align__(16) double Bs[2][kGK][kGN];
+// One FP64 tensor-core MMA (m8n8k4): d (8 x 8) += a (8 x 4) b (4 x 8).  Lane l
+// holds a[l / 4][l % 4], b[l % 4][l / 4] and d[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// 64 x 64 output tile per block of four warps, each warp a 32 x 32 quadrant
+// as 4 x 4 FP64 MMAs (m8n8k4) per k-step of 4.  A tiles (operator rows) are
+// copied as they lie (k-major), B tiles (one column per source cell) one
+// column per thread; rows of both are padded to 68 doubles so that every
+// fragment load of a warp is conflict-free.  The next 16-source chunk is
+// loaded into registers while the current one is multiplied from shared
+// memory (two buffers, one barrier per chunk).  Every output is a fixed-order
+// sum, so the result does not depend on the grid.
+__global__ void __launch_bounds__(kLThreads, 3) level_gemm(LevelGemm g) {
+  __shared__ __align__(16) double As[2][kGK][kLStride];
+  __shared__ __align__(16) double Bs[2][kGK][kLStride];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int r0 = blockIdx.y * kGM;
   const int64_t n0 = (int64_t)blockIdx.x * kGN;
-  const int wr = 32 * (w & 1) + 2 * (lane & 7);    // rows wr, wr+1, wr+16, wr+17
-  const int tc = 16 * (w >> 1) + 4 * (lane >> 3);  // columns tc .. tc+3
-  // A loads: rows r0 + 2 (tid & 31) (+1), sources (tid >> 5) and (tid >> 5) + 8
+  const int wm = 32 * (w & 1), wn = 32 * (w >> 1);  // the warp's quadrant
+  const int fr = lane >> 2, fk = lane & 3;            // fragment row / k of this lane
+  // A loads: rows r0 + 2 (tid & 31) (+1), sources (tid >> 5) + 4x, x < 4
   const int am = 2 * (tid & 31), ak = tid >> 5;
   const bool arow_ok = r0 + am < g.R;  // R even: the pair is valid together
-  // B loads: column tid & 63, sources 4 (tid >> 6) .. +3
-  const int bn = tid & 63, bk = 4 * (tid >> 6);
+  // B loads: column tid & 63, sources 8 (tid >> 6) .. +7
+  const int bn = tid & 63, bk = 8 * (tid >> 6);
   const int64_t bcol_i = n0 + bn;
   const bool bcol_ok = bcol_i < g.ncols;
   const double *bcol = nullptr;
@@ -789,13 +801,13 @@ __global__ void __launch_bounds__(kGThreads, 3) level_gemm(LevelGemm g) {
   }
   const int cps = (seg_len + kGK - 1) / kGK;  // chunks per segment
   const int nchunks = nseg * cps;
-  double2 av[2], bv[2];
+  double2 av[4], bv[4];
   auto load_chunk = [&](int c) {
     const int sg = seg0 + c / cps, kc = (c % cps) * kGK;
     const int kseg = seg_k0 + sg * g.nt2;  // first source of the segment
 #pragma unroll
-    for (int x = 0; x < 2; x++) {
-      const int kk = kc + ak + 8 * x;
+    for (int x = 0; x < 4; x++) {
+      const int kk = kc + ak + 4 * x;
       av[x] = (kk < seg_len && arow_ok)
                   ? *reinterpret_cast<const double2 *>(g.At + (size_t)(kseg + kk) * g.R + r0 + am)
                   : make_double2(0, 0);
@@ -804,56 +816,52 @@ __global__ void __launch_bounds__(kGThreads, 3) level_gemm(LevelGemm g) {
                                         : make_double2(0, 0);
     }
   };
-  double acc[4][4];
+  double acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0;
+    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0;
   if (nchunks > 0) load_chunk(0);
   for (int c = 0; c < nchunks; c++) {
     const int buf = c & 1;
 #pragma unroll
-    for (int x = 0; x < 2; x++) {
-      *reinterpret_cast<double2 *>(&As[buf][ak + 8 * x][am]) = av[x];
+    for (int x = 0; x < 4; x++) {
+      *reinterpret_cast<double2 *>(&As[buf][ak + 4 * x][am]) = av[x];
       Bs[buf][bk + 2 * x][bn] = bv[x].x;
       Bs[buf][bk + 2 * x + 1][bn] = bv[x].y;
     }
     __syncthreads();
     if (c + 1 < nchunks) load_chunk(c + 1);
 #pragma unroll
-    for (int k = 0; k < kGK; k++) {
-      const double2 a01 = *reinterpret_cast<const double2 *>(&As[buf][k][wr]);
-      const double2 a23 = *reinterpret_cast<const double2 *>(&As[buf][k][wr + 16]);
-      const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc]);
-      const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[buf][k][tc + 2]);
-      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
-      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+    for (int k0 = 0; k0 < kGK; k0 += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[buf][k0 + fk][wm + 8 * i + fr];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[buf][k0 + fk][wn + 8 * j + fr];
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; j++) dmma_m8n8k4(acc[i][j], a[i], b[j]);
     }
   }
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    const int64_t ci = n0 + tc + j;
-    if (ci >= g.ncols) continue;
-    const int64_t child0 = g.c0 + 8 * ci;
-    double *ccol;
-    if (g.split) ccol = g.part + ((int64_t)blockIdx.z * g.ncols + ci) * g.R;
-    else ccol = g.X + (g.up ? (int64_t)g.cparent[child0] : child0) * g.nt2;
 #pragma unroll
-    for (int i = 0; i < 4; i += 2) {
-      const int row = r0 + wr + 8 * i;  // wr, then wr + 16; even, R is even
-      if (row >= g.R) continue;
-      double2 *dst = reinterpret_cast<double2 *>(ccol + row);
-      double2 v = make_double2(acc[i][j], acc[i + 1][j]);
-      if (!g.up) {
-        const double2 o = *dst;
-        v.x += o.x;
-        v.y += o.y;
+    for (int e = 0; e < 2; e++) {
+      const int64_t ci = n0 + wn + 8 * j + 2 * fk + e;
+      if (ci >= g.ncols) continue;
+      const int64_t child0 = g.c0 + 8 * ci;
+      double *ccol;
+      if (g.split) ccol = g.part + ((int64_t)blockIdx.z * g.ncols + ci) * g.R;
+      else ccol = g.X + (g.up ? (int64_t)g.cparent[child0] : child0) * g.nt2;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int row = r0 + wm + 8 * i + fr;
+        if (row >= g.R) continue;
+        if (g.up) ccol[row] = acc[i][j][e];
+        else ccol[row] += acc[i][j][e];
       }
-      *dst = v;
     }
   }
 }
@@ -1166,7 +1174,7 @@ int level_translate(tapas_b200_ctx *ctx, int l, const LevelFirstChild &lf, bool 
     g.part = ctx->op_part.p;
     grid.z = 8;
   }
-  level_gemm<<<grid, kGThreads, 0, ctx->stream>>>(g);
+  level_gemm<<<grid, kLThreads, 0, ctx->stream>>>(g);
   TB_LAUNCH_CHECK(ctx);
   if (g.split) {
     sum_octant_parts<<<grid_for(ncols * g.R, 256), 256, 0, ctx->stream>>>(
