@@ -1269,7 +1269,9 @@ int m2l_gemm64_P(tapas_b200_ctx *ctx) {
   M2LClassInfo ci;
   {
     PhaseTimer t(ctx, &ctx->timings.m2l_setup);
-    TB_TRY(m2l_classes(ctx, sizeof(double) * (size_t)K * K, ci));
+    // classes of at least 32 pairs: smaller ones cost more as one GEMM launch
+    // each than on the pair kernel
+    TB_TRY(m2l_classes(ctx, sizeof(double) * (size_t)K * K, 32, ci));
     if (ci.ntc > 0) {
       TB_CUDA(ctx, T.ops64.ensure((size_t)K * K * ci.ntc, s));
       build_operators64<P><<<(unsigned)ci.ntc, 256, 0, s>>>(T.tc_keys.p, T.ops64.p);

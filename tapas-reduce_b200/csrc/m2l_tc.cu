@@ -992,7 +992,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
 // classes' wide keys (tc_keys), (first sorted pair, pair count) (cls_range)
 // and 128-pair tiles (items), and the list indices of the pairs left to the
 // FP64 pair path (pairs64).
-int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, M2LClassInfo &info) {
+int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, int64_t min_pairs, M2LClassInfo &info) {
   cudaStream_t s = ctx->stream;
   info = M2LClassInfo{};
   int64_t n = ctx->n_m2l;  // pairs to evaluate here (sharded: of owned targets)
@@ -1058,7 +1058,7 @@ int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, M2LClassInfo &info) {
   TB_LAUNCH_CHECK(ctx);
   // Operator memory is bounded: when more classes qualify than the budget
   // holds, only the most populated ones run on the tensor cores.
-  int64_t min_count = kTcMin;
+  int64_t min_count = min_pairs;
   {
     const int64_t max_classes = std::max<int64_t>(1, (int64_t)(ctx->tc_op_budget / op_bytes));
     if (nseg > max_classes) {
@@ -1070,7 +1070,7 @@ int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, M2LClassInfo &info) {
       for (int64_t c = 0; c < nseg; c++) cnt[c] = (c + 1 < nseg ? st[c + 1] : n) - st[c];
       std::nth_element(cnt.begin(), cnt.begin() + (max_classes - 1), cnt.end(),
                        std::greater<int64_t>());
-      min_count = std::max<int64_t>(kTcMin, cnt[max_classes - 1] + 1);
+      min_count = std::max<int64_t>(min_pairs, cnt[max_classes - 1] + 1);
     }
   }
   class_tc_flags<<<grid_for(nseg, 256), 256, 0, s>>>(T.seg_start.p, nseg, n, T.keys.p, kp,
@@ -1161,7 +1161,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   std::optional<PhaseTimer> setup_timer;
   setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
   M2LClassInfo ci;
-  TB_TRY(m2l_classes(ctx, sizeof(float) * (size_t)S::OPS_FLOATS, ci));
+  TB_TRY(m2l_classes(ctx, sizeof(float) * (size_t)S::OPS_FLOATS, kTcMin, ci));
   if (n == 0) {  // no M2L pair: every local expansion is zero
     TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
     TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));

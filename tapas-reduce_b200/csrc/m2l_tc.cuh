@@ -23,11 +23,11 @@ struct M2LClassInfo {
   int64_t n64 = 0;     // pairs left to the FP64 pair path (list indices in ctx->tc.pairs64)
 };
 // Classifies and sorts the M2L pairs by offset class and selects the classes
-// with at least 32 pairs, at most as many as ctx->tc_op_budget bytes of
+// with at least min_pairs pairs, at most as many as ctx->tc_op_budget bytes of
 // operators of op_bytes each hold (the most populated first).  Fills
 // ctx->tc: vals (list indices sorted by class), tc_keys (selected classes'
 // keys: delta + 32 in bits 42-47, D_z, D_y, D_x + 8192 in 14 bits each),
 // cls_range (first sorted pair, pair count), items (128-pair tiles) and
 // pairs64; err[1] = pairs in selected classes.
-int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, M2LClassInfo &info);
+int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, int64_t min_pairs, M2LClassInfo &info);
 }  // namespace tb
