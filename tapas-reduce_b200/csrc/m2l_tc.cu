@@ -1293,6 +1293,20 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
   }
 }
 
+// One level's 128-pair tiles: per_octant tiles of each octant's np pairs.
+__global__ void tree_tiles(int64_t np, int64_t per_octant, TileItem *__restrict__ items) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 8 * per_octant;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = e / per_octant, st = (e - o * per_octant) * kNTile;
+    TileItem it;
+    it.cls = (int32_t)o;
+    it.start = (int32_t)(o * np + st);
+    it.len = (int32_t)(np - st < kNTile ? np - st : kNTile);
+    it.pad = 0;
+    items[e] = it;
+  }
+}
+
 // The (parent, child) pairs of one level's M2M, octant-major: entry o * np + i
 // is parent i's octant o.  c0: the level's first child.
 __global__ void tree_pairs(int64_t c0, int64_t np, const int32_t *__restrict__ cparent,
@@ -1350,24 +1364,12 @@ int tree_level_gemm(tapas_b200_ctx *ctx, int64_t c0, int64_t np, const float *ro
   auto &T = ctx->tc;
   tree_pairs<<<grid_for(8 * np, 256), 256, 0, s>>>(c0, np, ctx->cparent.p, T.tree_list.p);
   TB_LAUNCH_CHECK(ctx);
-  std::vector<TileItem> items;
-  items.reserve((size_t)(8 * ((np + kNTile - 1) / kNTile)));
-  for (int o = 0; o < 8; o++)
-    for (int64_t st = 0; st < np; st += kNTile) {
-      TileItem it;
-      it.cls = o;
-      it.start = (int32_t)(o * np + st);
-      it.len = (int32_t)std::min<int64_t>(kNTile, np - st);
-      it.pad = 0;
-      items.push_back(it);
-    }
-  const int64_t nitems = (int64_t)items.size();
+  const int64_t per_octant = (np + kNTile - 1) / kNTile;
+  const int64_t nitems = 8 * per_octant;
   TB_CUDA(ctx, T.tree_items.ensure((size_t)nitems * sizeof(TileItem) / 16 + 1, s));
-  TB_CUDA(ctx, ctx->pinned.ensure(sizeof(TileItem) * (size_t)nitems + 256));
-  memcpy(ctx->pinned.p, items.data(), sizeof(TileItem) * (size_t)nitems);
-  TB_CUDA(ctx, cudaMemcpyAsync(T.tree_items.p, ctx->pinned.p, sizeof(TileItem) * (size_t)nitems,
-                               cudaMemcpyHostToDevice, s));
-  TB_CUDA(ctx, cudaStreamSynchronize(s));  // the pinned staging buffer is reused
+  tree_tiles<<<grid_for(nitems, 256), 256, 0, s>>>(np, per_octant,
+                                                    reinterpret_cast<TileItem *>(T.tree_items.p));
+  TB_LAUNCH_CHECK(ctx);
   static_assert(S::SMEM <= 227 * 1024 - 4096, "shared memory");
   TB_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<P, true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
