@@ -18,9 +18,11 @@ arithmetic form, mixed or FP64):
   P=14 -> 1.3e-6, P=16 -> 7.5e-7); the fixed fallback is P=10, theta=0.4,
   ncrit=64, FP64 (the reference's default setting).
 
-``evaluate_verified`` runs the chosen setting, checks it against an FP64
-direct sum on sampled targets, and falls back to the fixed setting when the
-check misses the tolerance.
+``evaluate_verified`` runs the learned chooser's shortlist (the fastest
+candidates predicted to meet the tolerance, then the margin-safe choice),
+checks each against an FP64 direct sum on sampled targets, times the ones that
+meet it and keeps the fastest; the fixed setting is the fallback when none
+meets it.
 """
 from __future__ import annotations
 
@@ -132,7 +134,7 @@ class LearnedChooser:
                 "precision": "fp64" if f64 else "mixed", "source": src,
                 "pred_log10_err": float(pred[idx, 0]), "pred_log10_ms": float(pred[idx, 1])}
 
-    def ranked(self, features: np.ndarray, tol: float, precisions=(0, 1), k: int = 3) -> list:
+    def ranked(self, features: np.ndarray, tol: float, precisions=(0, 1), k: int = 4) -> list:
         """Settings to try in order, for a caller that verifies each one: up to
         k - 1 of the fastest candidates predicted to meet `tol` without the
         safety margin, then the margin-safe choice of `choose`."""
@@ -188,7 +190,7 @@ def choose_params(n: int, tol: float, precision: str = "mixed", features=None,
     return dict(FIXED, source="fixed")
 
 
-def candidates(ctx, features, n: int, tol: float, precision: str = "auto", k: int = 3) -> list:
+def candidates(ctx, features, n: int, tol: float, precision: str = "auto", k: int = 4) -> list:
     """Settings to verify in order: the learned chooser's ranked candidates
     when a model is present, else the rule table's setting."""
     lc = learned_chooser(ctx) if (ctx is not None and features is not None) else None
@@ -198,11 +200,13 @@ def candidates(ctx, features, n: int, tol: float, precision: str = "auto", k: in
     return [choose_params(n, tol, precision)]
 
 
-def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=None, k=3):
+def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=None, k=4):
     """Chosen settings -> evaluation -> FP64 direct-sum check on `targets`:
-    the learned chooser's candidates are tried in order (at most k) and the
-    first that meets `tol` is kept; the fixed setting is the fallback when
-    none does.  Returns (results, info)."""
+    each of the learned chooser's candidates (at most k) is run, checked and
+    timed (device time of a second evaluation), and the fastest that meets
+    `tol` is kept, so the model's timing error (about 20 %) does not decide
+    between settings whose predicted times are that close; the fixed setting
+    is the fallback when none meets it.  Returns (results, info)."""
     from importlib import import_module
     rel_l2 = import_module("tapas_reduce_b200.verify").rel_l2
     if params is None:
@@ -213,6 +217,7 @@ def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=N
         tries = [params]
     d = None
     tried = []
+    best = None  # (ms, params, res, err)
     for params in tries:
         prec = tb.FP64 if params["precision"] == "fp64" else tb.MIXED
         res = ctx.evaluate(x, y, z, q, P=params["P"], ncrit=params["ncrit"],
@@ -220,9 +225,15 @@ def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=N
         if d is None:
             d = ctx.direct(targets)
         err = rel_l2(res[targets], d)
-        tried.append({"params": params, "rel_l2_pot": err[0]})
+        rec = {"params": params, "rel_l2_pot": err[0]}
         if err[0] <= tol:
-            break
+            ms = measured_ms(ctx, x, y, z, q, params, prec) if len(tries) > 1 else None
+            rec["ms"] = ms
+            if best is None or (ms is not None and ms < best[0]):
+                best = (ms, params, res, err)
+        tried.append(rec)
+    if best is not None:
+        _, params, res, err = best
     info = {"params": params, "rel_l2_pot": err[0], "rel_l2_acc": err[1],
             "met": err[0] <= tol, "fallback": False, "tried": tried}
     if not info["met"]:
@@ -232,3 +243,21 @@ def evaluate_verified(tb, ctx, x, y, z, q, tol, targets, params=None, features=N
         info.update(fallback=True, fallback_rel_l2_pot=err[0], fallback_rel_l2_acc=err[1],
                     fallback_met=err[0] <= tol)
     return res, info
+
+
+# The phases a step's device time is summed over.
+_PHASES = ("bbox_keys", "sort", "tree", "upward", "traverse", "list_sort", "m2l", "p2p",
+           "downward")
+
+
+def measured_ms(ctx, x, y, z, q, params, prec) -> float:
+    """Device milliseconds of one evaluation with `params` (the sum of the
+    library's CUDA-event phase timings; the caller has run it once already)."""
+    ctx.set_profiling(True)
+    try:
+        ctx.evaluate(x, y, z, q, P=params["P"], ncrit=params["ncrit"], theta=params["theta"],
+                     precision=prec)
+        t = ctx.timings()
+    finally:
+        ctx.set_profiling(False)
+    return float(sum(t[k] for k in _PHASES))
