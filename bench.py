@@ -177,9 +177,10 @@ def replica_throughput(pg, ms: float, n: int):
 # ---------------------------------------------------------------------------
 REF_SAMPLE_N = 50_000
 # The setting the reference runs on its samples: the one the learned chooser
-# picks for the 16M sphere-surface workload (and the sampled reference output
-# of that workload was made with), so both arms evaluate the same method.
-REF_P, REF_THETA, REF_NCRIT = 15, 0.4, 128
+# picks for the 16M sphere-surface workload (and one of the sampled reference
+# outputs of that workload was made with), so both arms evaluate the same
+# method.
+REF_P, REF_THETA, REF_NCRIT = 13, 0.35, 128
 GOLDEN = ROOT / "tests" / "golden"
 
 
@@ -229,11 +230,13 @@ def reference_scaling_evidence():
     setting) at the sizes its sampled outputs were made at: it shows how the
     bounded-sample rate carries to the full workload."""
     out = {}
-    for name in ("refsample_sphere_n1000000_p15", "refsample_sphere_n16000000_p15"):
+    for name in ("refsample_sphere_n1000000_p15", "refsample_sphere_n16000000_p15",
+                 "refsample_sphere_n16000000_p13"):
         f = GOLDEN / f"{name}.npz"
         if f.exists():
             g = np.load(f)
-            out[f"n{int(g['n'])}"] = _r(int(g["n"]) / float(g["ref_seconds"]))
+            key = f"n{int(g['n'])}_P{int(g['P'])}_theta{float(g['theta']):g}"
+            out[key] = _r(int(g["n"]) / float(g["ref_seconds"]))
     return out
 
 
@@ -243,7 +246,8 @@ def cpu_baseline_obj(value, kind, secs, n=REF_SAMPLE_N, cores=1):
            f"each on its own sample of {n} bodies")
     return {"value": value, "unit": "particles/s", "cores": cores, "kind": kind,
             "sample": f"{n} bodies of the same sphere-surface workload, "
-                      f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (the timed setting), "
+                      f"P={REF_P} theta={REF_THETA} ncrit={REF_NCRIT} (the setting the "
+                      f"chooser picks for this workload), "
                       f"{who}, {secs:.2f} s",
             "ref_rate_at_full_sizes_1core": reference_scaling_evidence()}
 
@@ -505,12 +509,20 @@ def main():
     err = orc.rel_l2(res[tg], d_check)
     accuracy = {"rel_l2_pot": _r(err[0]), "rel_l2_acc": _r(err[1]), "targets": int(len(tg)),
                 "meets_tol": bool(err[0] <= args.tol)}
-    ref16 = reference_sample("refsample_sphere_n16000000_p15") if (n == 16_000_000 and
-                                                                     rank == 0) else None
-    if ref16 is not None and ref16[2] == (P, theta, ncrit):
+    ref16 = None
+    if n == 16_000_000 and rank == 0:  # the reference's output at our setting if made, else P=15
+        for name in ("refsample_sphere_n16000000_p13", "refsample_sphere_n16000000_p15"):
+            ref16 = reference_sample(name)
+            if ref16 is not None and ref16[2] == (P, theta, ncrit):
+                break
+    if ref16 is not None:
+        # the reference's FP64 output on the same bodies, at its own setting
+        # (P, theta, ncrit) = reference_setting; at another setting of ours the
+        # difference holds both evaluations' truncation errors
         e = rel_l2_pair(res[ref16[0]], ref16[1])
         accuracy.update(rel_l2_pot_vs_reference=_r(e[0]), rel_l2_acc_vs_reference=_r(e[1]),
-                        reference_samples=int(len(ref16[0])))
+                        reference_samples=int(len(ref16[0])),
+                        reference_setting=list(ref16[2]))
 
     # ---- e2e through the C-ABI call with pinned host buffers, K steps ----
     for _ in range(2):

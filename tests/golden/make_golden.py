@@ -100,6 +100,7 @@ SAMPLED_CASES = {
     "refsample_plummer_n1000000_p10": ("plummer", 1_000_000, 102, 10, 64, 0.4, 2000),
     "refsample_sphere_n1000000_p15": ("sphere_surface", 1_000_000, 104, 15, 128, 0.4, 4000),
     "refsample_sphere_n16000000_p15": ("sphere_surface", 16_000_000, 5, 15, 128, 0.4, 4000),
+    "refsample_sphere_n16000000_p13": ("sphere_surface", 16_000_000, 5, 13, 128, 0.35, 4000),
 }
 
 
