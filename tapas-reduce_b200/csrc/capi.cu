@@ -223,6 +223,9 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
     if (ctx->gemm_join[k]) cudaEventDestroy(ctx->gemm_join[k]);
   }
   if (ctx->gemm_fork) cudaEventDestroy(ctx->gemm_fork);
+  if (ctx->upload_stream) cudaStreamDestroy(ctx->upload_stream);
+  if (ctx->q_ready) cudaEventDestroy(ctx->q_ready);
+  if (ctx->upload_fork) cudaEventDestroy(ctx->upload_fork);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return TAPAS_B200_OK;
@@ -294,7 +297,26 @@ int tapas_b200_partition(tapas_b200_ctx *ctx, const double *x, const double *y, 
     TB_TRY(copy_in(ctx, ctx->x.p, x, n, mem));
     TB_TRY(copy_in(ctx, ctx->y.p, y, n, mem));
     TB_TRY(copy_in(ctx, ctx->z.p, z, n, mem));
+    ctx->q_pending = false;
+  }
+  if (mem == TAPAS_B200_DEVICE) {
+    PhaseTimer t(ctx, &ctx->timings.upload);
     TB_TRY(copy_in(ctx, ctx->q.p, q, n, mem));
+  } else {
+    // The charges are first read when the sorted bodies are gathered: their
+    // copy from the host runs on a side stream while the keys are built and
+    // sorted.
+    if (!ctx->upload_stream) {
+      TB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->upload_stream, cudaStreamNonBlocking));
+      TB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->q_ready, cudaEventDisableTiming));
+      TB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->upload_fork, cudaEventDisableTiming));
+    }
+    TB_CUDA(ctx, cudaEventRecord(ctx->upload_fork, s));  // q's buffer is free from here
+    TB_CUDA(ctx, cudaStreamWaitEvent(ctx->upload_stream, ctx->upload_fork, 0));
+    TB_CUDA(ctx, cudaMemcpyAsync(ctx->q.p, q, sizeof(double) * (size_t)n,
+                                 cudaMemcpyHostToDevice, ctx->upload_stream));
+    TB_CUDA(ctx, cudaEventRecord(ctx->q_ready, ctx->upload_stream));
+    ctx->q_pending = true;
   }
   ctx->n = n;
   ctx->have_bh_attr = false;

@@ -250,6 +250,10 @@ struct tapas_b200_ctx {
   cudaStream_t gemm_streams[tb::kGemmSlabs] = {};
   cudaEvent_t gemm_join[tb::kGemmSlabs] = {};
   cudaEvent_t gemm_fork = nullptr;
+  // upload of the charges on a side stream while the keys are built and sorted
+  cudaStream_t upload_stream = nullptr;
+  cudaEvent_t q_ready = nullptr, upload_fork = nullptr;
+  bool q_pending = false;  // q is being copied: pack it after waiting for q_ready
 };
 
 namespace tb {

@@ -79,7 +79,8 @@ __global__ void bbox_final(const double *__restrict__ part, int nparts, double *
 }
 
 // Keys of the bodies, and each body packed as one 32-byte record (x, y, z, q)
-// so the gather into key order reads one sector per body.
+// so the gather into key order reads one sector per body; with q null the
+// charge is packed later (pack_charges).
 __global__ void __launch_bounds__(kBlock) keys_kernel(const double *__restrict__ x,
                                                       const double *__restrict__ y,
                                                       const double *__restrict__ z,
@@ -103,8 +104,15 @@ __global__ void __launch_bounds__(kBlock) keys_kernel(const double *__restrict__
     }
     keys[i] = finest_key(a[0], a[1], a[2]);
     idx[i] = (uint32_t)i;
-    packed[i] = make_double4(p[0], p[1], p[2], q[i]);
+    packed[i] = make_double4(p[0], p[1], p[2], q ? q[i] : 0.0);
   }
+}
+
+__global__ void pack_charges(const double *__restrict__ q, int64_t n,
+                             double4 *__restrict__ packed) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    packed[i].w = q[i];
 }
 
 __global__ void __launch_bounds__(kBlock) gather_bodies(
@@ -303,8 +311,8 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
     bbox_final<<<1, 32, 0, s>>>(ctx->scratch_d.p, nparts, ctx->bbox.p);
     TB_LAUNCH_CHECK(ctx);
     keys_kernel<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-        ctx->x.p, ctx->y.p, ctx->z.p, ctx->q.p, n, ctx->bbox.p, ctx->keys.p, ctx->idx.p,
-        ctx->body_pack.p);
+        ctx->x.p, ctx->y.p, ctx->z.p, ctx->q_pending ? nullptr : ctx->q.p, n, ctx->bbox.p,
+        ctx->keys.p, ctx->idx.p, ctx->body_pack.p);
     TB_LAUNCH_CHECK(ctx);
   }
   {
@@ -315,6 +323,13 @@ int build_tree(tapas_b200_ctx *ctx, int ncrit) {
     TB_TRY(radix_sort(ctx, k, ka, v, va, n, kDepthBits, kDepthBits + 3 * kMaxDepth));
     if (k != ctx->keys.p) { std::swap(ctx->keys.p, ctx->keys_alt.p); std::swap(ctx->keys.cap, ctx->keys_alt.cap); }
     if (v != ctx->idx.p) { std::swap(ctx->idx.p, ctx->idx_alt.p); std::swap(ctx->idx.cap, ctx->idx_alt.cap); }
+    if (ctx->q_pending) {  // the charges' copy ran alongside the keys and the sort
+      TB_CUDA(ctx, cudaStreamWaitEvent(s, ctx->q_ready, 0));
+      pack_charges<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(ctx->q.p, n,
+                                                                            ctx->body_pack.p);
+      TB_LAUNCH_CHECK(ctx);
+      ctx->q_pending = false;
+    }
     gather_bodies<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
         ctx->body_pack.p, ctx->idx.p, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p);
     TB_LAUNCH_CHECK(ctx);
