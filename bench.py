@@ -6,10 +6,11 @@ dual-tree traversal with M2L + P2P, downward pass):
   N = 16,000,000 bodies uniform on the unit sphere surface, charges U[-1,1]
   minus their mean, requested relative-L2 potential error 1e-6.  Parameters
   (P, theta, ncrit) come from the learned chooser: its shortlist (the fastest
-  candidates predicted to meet the tolerance, then the margin-safe choice) is
-  verified against an FP64 direct sum on 4,000 sampled targets and the ones
-  that meet it are run once more, timed (all before the timed region); the
-  fastest of them is timed, the rule table's setting if none meets it.
+  candidates predicted to come within 0.25 in log10 of the tolerance, then the
+  margin-safe choice) is verified against an FP64 direct sum on 4,000 sampled
+  targets and the ones that meet it are run twice more, timed (all before the
+  timed region); the fastest of them is timed, the rule table's setting if
+  none meets it.
 
 Printed JSON line (rank 0):
   value       particles/s of the mixed form, inputs resident in HBM

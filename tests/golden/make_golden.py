@@ -101,6 +101,7 @@ SAMPLED_CASES = {
     "refsample_sphere_n1000000_p15": ("sphere_surface", 1_000_000, 104, 15, 128, 0.4, 4000),
     "refsample_sphere_n16000000_p15": ("sphere_surface", 16_000_000, 5, 15, 128, 0.4, 4000),
     "refsample_sphere_n16000000_p13": ("sphere_surface", 16_000_000, 5, 13, 128, 0.35, 4000),
+    "refsample_sphere_n16000000_p12": ("sphere_surface", 16_000_000, 5, 12, 128, 0.35, 4000),
 }
 
 
