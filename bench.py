@@ -181,7 +181,7 @@ REF_SAMPLE_N = 50_000
 # picks for the 16M sphere-surface workload (and one of the sampled reference
 # outputs of that workload was made with), so both arms evaluate the same
 # method.
-REF_P, REF_THETA, REF_NCRIT = 13, 0.35, 128
+REF_P, REF_THETA, REF_NCRIT = 12, 0.35, 128
 GOLDEN = ROOT / "tests" / "golden"
 
 
@@ -232,7 +232,7 @@ def reference_scaling_evidence():
     bounded-sample rate carries to the full workload."""
     out = {}
     for name in ("refsample_sphere_n1000000_p15", "refsample_sphere_n16000000_p15",
-                 "refsample_sphere_n16000000_p13"):
+                 "refsample_sphere_n16000000_p13", "refsample_sphere_n16000000_p12"):
         f = GOLDEN / f"{name}.npz"
         if f.exists():
             g = np.load(f)
@@ -512,7 +512,8 @@ def main():
                 "meets_tol": bool(err[0] <= args.tol)}
     ref16 = None
     if n == 16_000_000 and rank == 0:  # the reference's output at our setting if made, else P=15
-        for name in ("refsample_sphere_n16000000_p13", "refsample_sphere_n16000000_p15"):
+        for name in ("refsample_sphere_n16000000_p12", "refsample_sphere_n16000000_p13",
+                     "refsample_sphere_n16000000_p15"):
             ref16 = reference_sample(name)
             if ref16 is not None and ref16[2] == (P, theta, ncrit):
                 break

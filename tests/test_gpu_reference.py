@@ -10,9 +10,8 @@ built in oracle/_ref):
     CPU-runnable configuration);
   - 1M Plummer bodies at P=10, theta=0.4, ncrit=64;
   - 1M and 16M sphere-surface bodies (zero-mean charges) at P=15, theta=0.4,
-    ncrit=128, and the 16M set at P=13, theta=0.35, ncrit=128 (the settings the
-    learned chooser picked for the 16M workload, with its earlier and its
-    current training data);
+    ncrit=128, and the 16M set at P=13 and P=12 with theta=0.35, ncrit=128 (the
+    settings the learned chooser has picked for the 16M workload);
 * the small full-output fixtures, for the mixed form.
 Bars: FP64 form max relative difference <= 1e-11 of the reference's values;
 mixed form rel-L2 <= 2e-6 (potential and acceleration) against them.
@@ -27,7 +26,7 @@ pytestmark = pytest.mark.gpu
 GDIR = pathlib.Path(__file__).parent / "golden"
 SAMPLED = ["refsample_cube_n100000_p10", "refsample_plummer_n1000000_p10",
            "refsample_sphere_n1000000_p15", "refsample_sphere_n16000000_p15",
-           "refsample_sphere_n16000000_p13"]
+           "refsample_sphere_n16000000_p13", "refsample_sphere_n16000000_p12"]
 SMALL = sorted(p for p in GDIR.glob("*.npz")
                if not p.stem.startswith(("bh_", "refsample_", "mutual_", "io_")))
 
