@@ -122,6 +122,10 @@ struct TcState {
   int64_t iota_n = 0;
   DBuf<int4> tree_items;             // one level's 128-pair tiles
   bool mt_ready = false;             // Mt holds this tree's normalised split multipoles
+  // class-key field ranges (largest |offset|, |level difference|) of the last
+  // classification: the next one packs with them and checks that every pair fits
+  bool kp_cached = false;
+  int kp_bo = 0, kp_bd = 0;
   DBuf<int> err;
   void release() {
     keys.release(); keys_alt.release(); tc_keys.release(); vals.release(); vals_alt.release();

@@ -182,22 +182,48 @@ struct KeyPack {
   }
 };
 
+// Sort key per pair.  Also the pairs' field ranges (as class_ranges) into
+// ranges[0..1], and in *overflow the classed pairs outside kp's ranges (kp
+// taken from an earlier list); those get the FP64 code, and a nonzero count
+// means the keys must be rebuilt with the new ranges.
 __global__ void classify_pairs(int64_t n, const uint64_t *__restrict__ list, int shift,
                                const int32_t *__restrict__ cnb,
                                const int32_t *__restrict__ clevel,
                                const double *__restrict__ cmin, const double *__restrict__ cmax,
                                const double *__restrict__ ccen, KeyPack kp,
-                               uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+                               uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                               int *__restrict__ ranges, int *__restrict__ overflow) {
   const uint64_t mask = (1ull << shift) - 1;
+  int md = 0, ml = 0, over = 0;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
        e += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t v = list[e];
     int delta = 0;
     long long D[3];
-    const int kind =
+    int kind =
         pair_class((int)(v >> shift), (int)(v & mask), cnb, clevel, cmin, cmax, ccen, delta, D);
+    if (kind == 2) {
+      const int d = (int)max(llabs(D[0]), max(llabs(D[1]), llabs(D[2])));
+      md = max(md, d);
+      ml = max(ml, abs(delta));
+      if (d > kp.bo || abs(delta) > kp.bd) {
+        kind = 1;
+        over++;
+      }
+    }
     keys[e] = kind == 0 ? kp.empty() : (kind == 1 ? kp.rare() : kp.pack(delta, D));
     vals[e] = (uint32_t)e;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    md = max(md, __shfl_xor_sync(0xffffffffu, md, o));
+    ml = max(ml, __shfl_xor_sync(0xffffffffu, ml, o));
+    over += __shfl_xor_sync(0xffffffffu, over, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(ranges, md);
+    atomicMax(ranges + 1, ml);
+    if (over) atomicAdd(overflow, over);
   }
 }
 
@@ -1004,34 +1030,52 @@ int m2l_classes(tapas_b200_ctx *ctx, size_t op_bytes, int64_t min_pairs, M2LClas
   TB_CUDA(ctx, T.vals_alt.ensure(n + 1, s));
   TB_CUDA(ctx, T.pairs64.ensure(n + 1, s));
   if (n == 0) return TAPAS_B200_OK;
-  // key width from the lists' largest offsets
-  TB_CUDA(ctx, T.err.ensure(4, s));
-  TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 4 * sizeof(int), s));
-  class_ranges<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
-      n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
-      ctx->ccen.p, T.err.p + 2);
-  TB_LAUNCH_CHECK(ctx);
+  // Key width from the lists' largest offsets.  The ranges of the previous
+  // classification are tried first (classify_pairs reports the current ranges
+  // and the pairs that do not fit); only a first call or a miss runs the
+  // separate range pass.
+  TB_CUDA(ctx, T.err.ensure(8, s));
   TB_CUDA(ctx, ctx->pinned.ensure(256));
   int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
-  TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p + 2, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  TB_CUDA(ctx, cudaStreamSynchronize(s));
   KeyPack kp;
-  {
+  for (bool fresh = !T.kp_cached;; fresh = true) {
+    TB_CUDA(ctx, cudaMemsetAsync(T.err.p, 0, 8 * sizeof(int), s));
+    if (fresh) {
+      class_ranges<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+          n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
+          ctx->ccen.p, T.err.p + 2);
+      TB_LAUNCH_CHECK(ctx);
+      TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p + 2, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   s));
+      TB_CUDA(ctx, cudaStreamSynchronize(s));
+      T.kp_bo = h[0];
+      T.kp_bd = h[1];
+      T.kp_cached = true;
+    }
     auto bits_for = [](int64_t range) {  // bits holding 0..range
       int b = 1;
       while (((int64_t)1 << b) <= range) b++;
       return b;
     };
-    kp.bo = h[0];
-    kp.bd = h[1];
-    kp.cb = bits_for(2 * (int64_t)h[0]);
-    kp.db = bits_for(2 * (int64_t)h[1]);
+    kp.bo = T.kp_bo;
+    kp.bd = T.kp_bd;
+    kp.cb = bits_for(2 * (int64_t)kp.bo);
+    kp.db = bits_for(2 * (int64_t)kp.bd);
     kp.bits = kp.db + 3 * kp.cb + 1;
+    classify_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
+        n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
+        ctx->ccen.p, kp, T.keys.p, T.vals.p, T.err.p + 4, T.err.p + 6);
+    TB_LAUNCH_CHECK(ctx);
+    if (fresh) break;
+    TB_CUDA(ctx, cudaMemcpyAsync(h, T.err.p + 4, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    TB_CUDA(ctx, cudaStreamSynchronize(s));
+    if (h[2] == 0) {
+      // every pair fits; the next classification packs with this list's ranges
+      T.kp_bo = h[0];
+      T.kp_bd = h[1];
+      break;
+    }
   }
-  classify_pairs<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, s>>>(
-      n, ctx->m2l.p, ctx->list_shift, ctx->cnb.p, ctx->clevel.p, ctx->cmin.p, ctx->cmax.p,
-      ctx->ccen.p, kp, T.keys.p, T.vals.p);
-  TB_LAUNCH_CHECK(ctx);
   {
     uint64_t *k = T.keys.p, *ka = T.keys_alt.p;
     uint32_t *v = T.vals.p, *va = T.vals_alt.p;

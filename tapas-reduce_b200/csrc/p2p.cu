@@ -483,8 +483,7 @@ __device__ __forceinline__ void mixed_tile(
       {
         // far bodies: plain FP32 coordinates in the target frame (relative
         // error of a separation <= ~2.4e-7), no r = 0 case
-#pragma unroll 2
-        for (int k = gs; k < nfar; k += G) {
+        auto far_src = [&](int k) {
           const float4 bh = ss[wi][k].hi;
 #pragma unroll
           for (int r = 0; r < kR; r++) {
@@ -498,6 +497,14 @@ __device__ __forceinline__ void mixed_tile(
             ty[r] = fmaf(dy, qr3, ty[r]);
             tz[r] = fmaf(dz, qr3, tz[r]);
           }
+        };
+        if (G == 1) {
+          // one group takes every source: unit stride, fixed offsets
+#pragma unroll 4
+          for (int k = active ? 0 : nfar; k < nfar; k++) far_src(k);
+        } else {
+#pragma unroll 2
+          for (int k = gs; k < nfar; k += G) far_src(k);
         }
       }
       if (nfar < cnt) {

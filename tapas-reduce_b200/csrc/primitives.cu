@@ -144,8 +144,10 @@ int scan_exclusive(tapas_b200_ctx *ctx, const int32_t *in, int32_t *out, int64_t
 // Per pass (8-bit digit): (1) per-tile digit histogram, stored digit-major
 // [256][ntiles]; (2) one block per digit scans its row over tiles, and the
 // digit totals are scanned inside (3); (3) each tile ranks its elements
-// stably with warp match-any, sorts them by digit in shared memory and writes
-// them out as contiguous runs.
+// stably (the lanes sharing a digit found with one warp ballot per digit
+// bit), sorts them by digit in shared memory and writes them out as
+// contiguous runs; its keys are loaded before the digit bases, so the two
+// sets of loads overlap.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -234,6 +236,16 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
+  // this thread's keys (and values), in flight during the digit-base loads
+  const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
+  uint64_t k[kSortItems];
+  uint32_t v[kSortItems];
+#pragma unroll
+  for (int it = 0; it < kSortItems; it++) {
+    const int64_t g = tile0 + (int64_t)warp * (32 * kSortItems) + it * 32 + lane;
+    k[it] = g < n ? keys_in[g] : ~0ull;
+    if (kHasVals) v[it] = g < n ? vals_in[g] : 0u;
+  }
 
   // Global base per digit = exclusive scan of totals + this tile's row offset.
   if (threadIdx.x < 32) {
@@ -263,21 +275,20 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(
 
   // Warp-striped ownership: item k of lane l in warp w is tile element
   // w*(32*kSortItems) + k*32 + l, so (warp, round, lane) is input order.
-  const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
-  uint64_t k[kSortItems];
-  uint32_t v[kSortItems];
   uint32_t rank[kSortItems];
   const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int it = 0; it < kSortItems; it++) {
     int64_t g = tile0 + (int64_t)warp * (32 * kSortItems) + it * 32 + lane;
     bool valid = g < n;
-    k[it] = valid ? keys_in[g] : ~0ull;
-    if (kHasVals) v[it] = valid ? vals_in[g] : 0u;
     uint32_t d = valid ? digit_of(k[it], shift) : 0xFFFFFFFFu;
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    peers &= vmask;
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < kRadixBits; b++) {
+      const bool bit = (d >> b) & 1u;
+      const unsigned bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
     if (valid) {
       uint32_t before = wcnt[warp * kRadix + d];
       rank[it] = before + __popc(peers & lt_mask);
