@@ -335,6 +335,7 @@ int tapas_b200_get_device_view(tapas_b200_ctx *ctx, tapas_b200_device_view *out)
     set_error(ctx, "get_device_view: no tree (call partition first)");
     return TAPAS_B200_ERR_STATE;
   }
+  TB_TRY(sort_m2l_sources(ctx));  // the view's lists: sources in order per target
   *out = tapas_b200_device_view{};
   out->n_bodies = ctx->n;
   out->n_cells = ctx->ncells;
@@ -657,6 +658,7 @@ int tapas_b200_get_lists(tapas_b200_ctx *ctx, int32_t *m2l_tgt, int32_t *m2l_src
     set_error(ctx, "get_lists: no lists");
     return TAPAS_B200_ERR_STATE;
   }
+  TB_TRY(sort_m2l_sources(ctx));
   const int b = ctx->list_shift;
   const uint64_t mask = (1ull << b) - 1;
   for (int which = 0; which < 2; which++) {
@@ -685,8 +687,12 @@ int tapas_b200_m2l(tapas_b200_ctx *ctx, int precision) {
     return TAPAS_B200_ERR_STATE;
   }
   PhaseTimer t(ctx, &ctx->timings.m2l);
-  if (precision == TAPAS_B200_MIXED) TB_TRY(m2l_tensorcore(ctx));
-  else TB_TRY(m2l_fp64(ctx));
+  if (precision == TAPAS_B200_MIXED) {
+    TB_TRY(m2l_tensorcore(ctx));
+  } else {
+    TB_TRY(sort_m2l_sources(ctx));  // the FP64 sums run in source order
+    TB_TRY(m2l_fp64(ctx));
+  }
   ctx->have_L = true;
   return TAPAS_B200_OK;
 }
@@ -705,7 +711,11 @@ int tapas_b200_p2p(tapas_b200_ctx *ctx, int precision) {
 }
 
 int tapas_b200_traverse(tapas_b200_ctx *ctx, double theta, int mutual, int precision) {
-  TB_TRY(tapas_b200_build_lists(ctx, theta, mutual));
+  TB_TRY(check_ctx(ctx));
+  TB_TRY(check_precision(ctx, precision));
+  // the mixed M2L regroups its pairs by offset class: it needs the list
+  // grouped by target, not each target's sources sorted
+  TB_TRY(build_lists(ctx, theta, mutual, precision != TAPAS_B200_MIXED));
   TB_TRY(tapas_b200_m2l(ctx, precision));
   return tapas_b200_p2p(ctx, precision);
 }

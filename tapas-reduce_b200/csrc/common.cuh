@@ -107,7 +107,7 @@ struct TcState {
   DBuf<uint32_t> vals, vals_alt;
   DBuf<uint32_t> pairs64;  // list indices of the pairs left to the FP64 kernel
   DBuf<int32_t> flag, scan, seg_start, tcflag, tcid, ntiles, tile_off;
-  DBuf<int4> items;
+  DBuf<int4> items, items_alt;
   DBuf<int2> cls_range;    // per selected class: first sorted pair, pair count
   DBuf<float> ops, Mt, Lt;  // per selected class its FP32 operator rows; FP32 rows of M, L
   DBuf<double> ops64, Mt64, Lt64;  // FP64 class GEMM (plain form)
@@ -195,6 +195,8 @@ struct tapas_b200_ctx {
 
   // ---- traversal lists ----
   bool have_lists = false;
+  bool m2l_sources_sorted = true;       // each M2L target's sources in increasing order
+  unsigned long long m2l_longest = 0;   // longest M2L target segment
   double theta = 0.4;
   tb::DBuf<int2> front_a, front_b;      // (target, source) pairs
   tb::DBuf<uint64_t> m2l, p2p;          // (target << 32 | source)

@@ -362,6 +362,30 @@ __global__ void build_tiles(const int32_t *__restrict__ seg_start, int64_t nseg,
   }
 }
 
+// Region of each tile: the octant (at tree level kRegionLevel) of its first
+// pair's target, as a sort key, with the tile's index as the value.
+constexpr int kRegionLevel = 2;
+__global__ void tile_regions(const TileItem *__restrict__ items, int64_t nitems,
+                             const uint32_t *__restrict__ sorted_vals,
+                             const uint64_t *__restrict__ list, int shift,
+                             const uint64_t *__restrict__ ckey, uint64_t *__restrict__ rkey,
+                             uint32_t *__restrict__ rval) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nitems;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(list[sorted_vals[items[i].start]] >> shift);
+    rkey[i] = (ckey[t] >> (kDepthBits + 3 * (kMaxDepth - kRegionLevel))) &
+              ((1u << (3 * kRegionLevel)) - 1);
+    rval[i] = (uint32_t)i;
+  }
+}
+
+__global__ void gather_items(const TileItem *__restrict__ in, const uint32_t *__restrict__ order,
+                             int64_t nitems, TileItem *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nitems;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[order[i]];
+}
+
 // ---------------------------------------------------------------------------
 // operators
 // ---------------------------------------------------------------------------
@@ -1227,6 +1251,27 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
     TB_LAUNCH_CHECK(ctx);
   }
   TB_CUDA(ctx, cudaMemsetAsync(T.Lt.p, 0, sizeof(float) * (size_t)C * S::KP, s));
+  // Tiles in region order (stable, so by class inside a region): the CTAs,
+  // which take consecutive tiles, then gather the multipole rows of one region
+  // of the tree at a time, and those stay in L2 across its classes instead of
+  // being read from HBM once per class.
+  if (nitems > 1) {
+    TB_CUDA(ctx, T.items_alt.ensure((size_t)(nitems + 1) * sizeof(TileItem) / 16 + 1, s));
+    uint64_t *rk = T.keys.p, *rka = T.keys_alt.p;
+    uint32_t *rv = reinterpret_cast<uint32_t *>(T.scan.p);
+    uint32_t *rva = reinterpret_cast<uint32_t *>(T.flag.p);
+    tile_regions<<<grid_for(nitems, 256), 256, 0, s>>>(
+        reinterpret_cast<const TileItem *>(T.items.p), nitems, T.vals.p, ctx->m2l.p,
+        ctx->list_shift, ctx->ckey.p, rk, rv);
+    TB_LAUNCH_CHECK(ctx);
+    TB_TRY(radix_sort(ctx, rk, rka, rv, rva, nitems, 0, 3 * kRegionLevel));
+    gather_items<<<grid_for(nitems, 256), 256, 0, s>>>(
+        reinterpret_cast<const TileItem *>(T.items.p), rv, nitems,
+        reinterpret_cast<TileItem *>(T.items_alt.p));
+    TB_LAUNCH_CHECK(ctx);
+    std::swap(T.items.p, T.items_alt.p);
+    std::swap(T.items.cap, T.items_alt.cap);
+  }
   setup_timer.reset();
   // 5. FP64 part (rare classes) writes L; the GEMM adds into Lt
   TB_TRY(m2l_fp64_pairs(ctx, T.pairs64.p, n64));

@@ -372,15 +372,74 @@ __global__ void __launch_bounds__(kLongThreads) sort_long_segments(
   }
 }
 
+// out[i] = c << b | src[i] over each target segment, sources in the order
+// the scatter left them (one warp per target).
+__global__ void __launch_bounds__(kSegWarps * 32) pack_segments(
+    const uint32_t *__restrict__ src, const int32_t *__restrict__ off, int64_t ncells, int b,
+    uint64_t *__restrict__ out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * kSegWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kSegWarps + warp; c < ncells; c += warps) {
+    const int32_t a0 = off[c], a1 = off[c + 1];
+    const uint64_t th = (uint64_t)c << b;
+    for (int32_t i = a0 + lane; i < a1; i += 32) out[i] = th | src[i];
+  }
+}
+
+__global__ void list_sources(const uint64_t *__restrict__ v, int64_t n, uint64_t mask,
+                             uint32_t *__restrict__ src) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    src[i] = (uint32_t)(v[i] & mask);
+}
+
 int bits_for(int64_t x) {
   int b = 1;
   while (((int64_t)1 << b) <= x) b++;
   return b;
 }
 
+// Sorts each target segment of list w (0: M2L, 1: P2P) by source, given the
+// sources in segment order in ctx->list_src and the longest segment.
+int sort_segment_sources(tapas_b200_ctx *ctx, int w, unsigned long long longest) {
+  cudaStream_t s = ctx->stream;
+  const int64_t C = ctx->ncells;
+  const int b = ctx->list_shift;
+  tb::DBuf<uint64_t> &L = w ? ctx->p2p : ctx->m2l;
+  const int32_t *off = w ? ctx->p2p_off.p : ctx->m2l_off.p;
+  TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p + 7, 0, sizeof(unsigned long long), s));
+  // the per-target cursors are spent: their buffer holds the long-segment list
+  sort_segments<<<grid_for(C, kSegWarps, ctx->num_sms * 8), kSegWarps * 32, 0, s>>>(
+      ctx->list_src.p, off, C, b, L.p, ctx->list_cnt.p, ctx->counters.p + 7);
+  TB_LAUNCH_CHECK(ctx);
+  if (longest > (unsigned long long)kWarpSegMax) {
+    sort_long_segments<<<ctx->num_sms, kLongThreads, 0, s>>>(ctx->list_src.p, off, b, L.p,
+                                                              ctx->list_cnt.p,
+                                                              ctx->counters.p + 7);
+    TB_LAUNCH_CHECK(ctx);
+  }
+  return TAPAS_B200_OK;
+}
+
 }  // namespace
 
-int build_lists(tapas_b200_ctx *ctx, double theta, int mutual) {
+int sort_m2l_sources(tapas_b200_ctx *ctx) {
+  if (!ctx->have_lists || ctx->m2l_sources_sorted) return TAPAS_B200_OK;
+  const int64_t n = ctx->n_m2l;
+  if (n > 0) {
+    cudaStream_t s = ctx->stream;
+    TB_CUDA(ctx, ctx->list_src.ensure(n + 1, s));
+    TB_CUDA(ctx, ctx->list_cnt.ensure(ctx->ncells + 1, s));
+    list_sources<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
+        ctx->m2l.p, n, (1ull << ctx->list_shift) - 1, ctx->list_src.p);
+    TB_LAUNCH_CHECK(ctx);
+    TB_TRY(sort_segment_sources(ctx, 0, ctx->m2l_longest));
+  }
+  ctx->m2l_sources_sorted = true;
+  return TAPAS_B200_OK;
+}
+
+int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_m2l_sources) {
   if (!ctx->have_tree) {
     set_error(ctx, "build_lists: no tree (call partition first)");
     return TAPAS_B200_ERR_STATE;
@@ -519,6 +578,8 @@ int build_lists(tapas_b200_ctx *ctx, double theta, int mutual) {
     TB_CUDA(ctx, cudaMemcpyAsync(hc + 5, ctx->counters.p + 5, 2 * sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, s));
     TB_CUDA(ctx, cudaStreamSynchronize(s));
+    ctx->m2l_longest = hc[5];
+    ctx->m2l_sources_sorted = true;
     // 2. counting sort by target, then each target's sources
     for (int w = 0; w < 2; w++) {
       tb::DBuf<uint64_t> &L = *lists[w];
@@ -528,18 +589,18 @@ int build_lists(tapas_b200_ctx *ctx, double theta, int mutual) {
         TB_CUDA(ctx, ctx->list_src.ensure(n + 1, s));
         TB_CUDA(ctx, cudaMemcpyAsync(ctx->list_cnt.p, offs[w]->p, sizeof(int32_t) * C,
                                      cudaMemcpyDeviceToDevice, s));
-        TB_CUDA(ctx, cudaMemsetAsync(ctx->counters.p + 7, 0, sizeof(unsigned long long), s));
         scatter_by_target<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
             L.p, n, ctx->list_cnt.p, ctx->list_src.p);
         TB_LAUNCH_CHECK(ctx);
-        // the per-target cursors are spent: their buffer holds the long-segment list
-        sort_segments<<<grid_for(C, kSegWarps, ctx->num_sms * 8), kSegWarps * 32, 0, s>>>(
-            ctx->list_src.p, offs[w]->p, C, b, L.p, ctx->list_cnt.p, ctx->counters.p + 7);
-        TB_LAUNCH_CHECK(ctx);
-        if (hc[5 + w] > (unsigned long long)kWarpSegMax) {
-          sort_long_segments<<<ctx->num_sms, kLongThreads, 0, s>>>(
-              ctx->list_src.p, offs[w]->p, b, L.p, ctx->list_cnt.p, ctx->counters.p + 7);
+        if (w == 0 && !sort_m2l_sources) {
+          // grouped by target only; sort_m2l_sources() completes the order
+          // when a caller needs it
+          pack_segments<<<grid_for(C, kSegWarps, ctx->num_sms * 8), kSegWarps * 32, 0, s>>>(
+              ctx->list_src.p, offs[w]->p, C, b, L.p);
           TB_LAUNCH_CHECK(ctx);
+          ctx->m2l_sources_sorted = false;
+        } else {
+          TB_TRY(sort_segment_sources(ctx, w, hc[5 + w]));
         }
       } else {
         TB_CUDA(ctx, ctx->list_alt.ensure(n + 1, s));
