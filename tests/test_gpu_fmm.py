@@ -268,6 +268,27 @@ def test_deterministic(tb, ctx):
     assert _rel(a, b) < 1e-7
 
 
+def test_mixed_traverse_lists_sorted_on_demand(tb, ctx):
+    """The mixed form's traversal leaves each M2L target's sources unsorted
+    (its M2L regroups the pairs by offset class); the list accessor and a
+    later FP64 M2L see them sorted, as build_lists gives them, so an FP64
+    evaluation after a mixed traversal equals a plain one bit for bit."""
+    x, y, z, q = tb.datasets.make("sphere_surface", 40000, 3)
+    fp64 = ctx.evaluate(x, y, z, q, P=6, ncrit=32, theta=0.4, precision=tb.FP64)
+    (mt0, ms0), (pt0, ps0) = ctx.lists()
+    ctx.upward(P=6, precision=tb.FP64)
+    ctx.traverse(0.4, 0, tb.MIXED)
+    (mt, ms), (pt, ps) = ctx.lists()
+    for a, b in ((mt, mt0), (ms, ms0), (pt, pt0), (ps, ps0)):
+        assert np.array_equal(a, b)
+    assert np.all(np.diff(mt.astype(np.int64) * (1 << 32) + ms) > 0)
+    ctx.traverse(0.4, 0, tb.MIXED)
+    ctx.m2l(tb.FP64)
+    ctx.p2p(tb.FP64)
+    ctx.downward(tb.FP64)
+    assert np.array_equal(ctx.results(), fp64)
+
+
 @pytest.mark.parametrize("n,ncrit", [(1, 64), (2, 1), (5, 2), (50, 64), (64, 64), (65, 64)])
 def test_small_and_root_leaf(n, ncrit, tb, ctx, oracle_mod):
     """Tiny inputs, including a root that is itself a leaf (which the reference
