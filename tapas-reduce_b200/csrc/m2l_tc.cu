@@ -23,7 +23,8 @@
 //  4. GEMM kernel, warp-specialised: a CTA takes tiles of 128 pairs of one
 //     class; producer warps stream the sources' FP32 multipole rows
 //     (cp.async, split into TF32 hi + lo in shared memory) and the operator's
-//     K chunks (bulk copies) through a shared-memory ring; one thread issues tcgen05.mma kind::tf32 (M=128
+//     K chunks (bulk copies of its hi and lo rows) through a shared-memory
+//     ring; one thread issues tcgen05.mma kind::tf32 (M=128
 //     pairs, N = the operator rows the chunk reaches, K=8) three times per
 //     k-step (hi*hi + lo*hi + hi*lo: split-precision "3xTF32", FP32
 //     accumulation in TMEM).  An output of degree j reads only sources of
@@ -417,8 +418,8 @@ __device__ __forceinline__ int op_offset(const int *co, int r, int c) {
 }
 
 // One block per tensor-core class: unit-offset singular harmonics (evalLocal,
-// :102-135) in FP64, then every real operator entry the GEMM reads, in FP32
-// (the GEMM splits it into TF32 hi + lo in shared memory).
+// :102-135) in FP64, then every real operator entry the GEMM reads, rounded to
+// FP32 and split into TF32 hi + lo (the class's hi rows, then its lo rows).
 template <int P>
 __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restrict__ tc_keys,
                                                        float *__restrict__ ops) {
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *op = ops + (size_t)cls * S::OPS_FLOATS;
+  float *op = ops + (size_t)cls * 2 * S::OPS_FLOATS;
   // one thread per complex (output, input) pair: its real 2 x 2 block
   for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // complex output / input
@@ -480,8 +481,12 @@ __global__ void __launch_bounds__(256) build_operators(const uint64_t *__restric
     }
     const double v[4] = {v00, v01, v10, v11};
 #pragma unroll
-    for (int e = 0; e < 4; e++)
-      op[op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1))] = (float)v[e];
+    for (int e = 0; e < 4; e++) {
+      const int o = op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1));
+      const float x = (float)v[e], hi = tf32_round(x);
+      op[o] = hi;
+      op[S::OPS_FLOATS + o] = tf32_round(x - hi);
+    }
   }
 }
 
@@ -751,11 +756,11 @@ constexpr int kThreadsTc = 32 * 25;
 //    ring: every producer cp.async-copies its share of the 128 gathered
 //    multipole rows (A, FP32; lanes of a warp cover whole row segments) and
 //    arrives on landed[stage] when they have landed; thread 0 bulk-copies
-//    the operator rows the chunk reaches (B, contiguous, hi and lo), which
-//    complete on full[stage].  A stage is refilled after the MMAs that read
-//    it commit to empty[stage].
-//  - the split warps (17-24) wait for landed[stage], split the rows into
-//    TF32 hi + lo in place and arrive on full[stage].
+//    the operator rows the chunk reaches (B, contiguous, split into TF32 hi
+//    and lo when they were built), which complete on landed[stage] too.  A
+//    stage is refilled after the MMAs that read it commit to empty[stage].
+//  - the split warps (17-24) wait for landed[stage], split the multipole
+//    rows into TF32 hi + lo in place and arrive on full[stage].
 //  - the MMA thread (warp 16, lane 0) waits for full[stage], issues the
 //    chunk's 3xTF32 MMAs into one of TBUF TMEM accumulators and commits them
 //    to empty[stage]; after a tile's last chunk it commits to tfull[buffer].
@@ -868,11 +873,12 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sB_hi = sA_hi + 2 * kNTile * S::KC;
       if (tid == 0) {
-        // the chunk's operator rows (the ones it reaches), FP32, into the hi area
-        const size_t boff = (size_t)cur_cls * S::OPS_FLOATS + (size_t)co_sh[kc];
+        // the chunk's operator rows (the ones it reaches), TF32 hi and lo
+        const size_t boff = (size_t)cur_cls * 2 * S::OPS_FLOATS + (size_t)co_sh[kc];
         const uint32_t bbytes = (uint32_t)(nr_sh[kc] * S::KC * sizeof(float));
-        mbar_expect_tx(&landed[st], bbytes);
+        mbar_expect_tx(&landed[st], 2 * bbytes);
         bulk_copy(sB_hi, ops + boff, bbytes, &landed[st]);
+        bulk_copy(sB_hi + S::NPAD * S::KC, ops + boff + S::OPS_FLOATS, bbytes, &landed[st]);
       }
 #pragma unroll
       for (int i = 0; i < NRT; i++) {
@@ -938,9 +944,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
     __syncwarp();
   } else if (warp >= kSplitWarp0) {
     // ---------------- split ----------------
-    // once a stage's FP32 multipole rows and operator rows have landed, the
-    // 256 threads split them into TF32 hi + lo in place (16 bytes at a time),
-    // then arrive on full[stage]
+    // once a stage's FP32 multipole rows (and its operator rows, split when
+    // they were built) have landed, the 256 threads split the multipole rows
+    // into TF32 hi + lo in place (16 bytes at a time), then arrive on
+    // full[stage]
     const int t = tid - kSplitWarp0 * 32;
     auto split4 = [](float *hi_p, float *lo_p) {
       const float4 x = *reinterpret_cast<const float4 *>(hi_p);
@@ -958,15 +965,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1) m2l_tc_kernel(
       if (!wait_phase(&landed[st], (uint32_t)((step / NS) & 1), abort, wait_limit)) break;
       float *sA_hi = base + (size_t)st * S::STAGE_FLOATS;
       float *sA_lo = sA_hi + kNTile * S::KC;
-      float *sB_hi = sA_lo + kNTile * S::KC;
-      float *sB_lo = sB_hi + S::NPAD * S::KC;
 #pragma unroll
       for (int i = 0; i < (kNTile * S::KC) / (4 * kSplitThreads); i++) {
         const int o = 4 * (t + i * kSplitThreads);
         split4(sA_hi + o, sA_lo + o);
       }
-      const int nb4 = nr_sh[kc] * S::KC / 4;
-      for (int i = t; i < nb4; i += kSplitThreads) split4(sB_hi + 4 * i, sB_lo + 4 * i);
       fence_async_smem();  // the split rows are visible to the tensor core
       mbar_arrive(&full[st]);
     }
@@ -1229,7 +1232,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   std::optional<PhaseTimer> setup_timer;
   setup_timer.emplace(ctx, &ctx->timings.m2l_setup);
   M2LClassInfo ci;
-  TB_TRY(m2l_classes(ctx, sizeof(float) * (size_t)S::OPS_FLOATS, kTcMin, ci));
+  TB_TRY(m2l_classes(ctx, 2 * sizeof(float) * (size_t)S::OPS_FLOATS, kTcMin, ci));
   if (n == 0) {  // no M2L pair: every local expansion is zero
     TB_CUDA(ctx, ctx->L.ensure((size_t)C * S::NT, s));
     TB_CUDA(ctx, cudaMemsetAsync(ctx->L.p, 0, sizeof(double2) * (size_t)C * S::NT, s));
@@ -1238,7 +1241,7 @@ int m2l_tc_P(tapas_b200_ctx *ctx) {
   const int64_t ntc = ci.ntc, nitems = ci.nitems, n64 = ci.n64;
   int32_t *h = reinterpret_cast<int32_t *>(ctx->pinned.p);
   if (ntc > 0) {
-    TB_CUDA(ctx, T.ops.ensure((size_t)S::OPS_FLOATS * ntc, s));
+    TB_CUDA(ctx, T.ops.ensure((size_t)2 * S::OPS_FLOATS * ntc, s));
     build_operators<P><<<(unsigned)ntc, 256, 0, s>>>(T.tc_keys.p, T.ops.p);
     TB_LAUNCH_CHECK(ctx);
   }
@@ -1354,7 +1357,7 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
     ord[t] = (unsigned char)k;
   }
   __syncthreads();
-  float *op = ops + (size_t)o * S::OPS_FLOATS;
+  float *op = ops + (size_t)o * 2 * S::OPS_FLOATS;
   for (int idx = threadIdx.x; idx < (S::NPAD / 2) * (S::KP / 2); idx += blockDim.x) {
     const int to = idx / (S::KP / 2), ti = idx % (S::KP / 2);  // target / source coefficient
     cd a{0, 0}, b{0, 0};  // target += a * source + b * conj(source)
@@ -1377,8 +1380,12 @@ __global__ void __launch_bounds__(256) build_tree_ops(const int32_t *__restrict_
     // [row re/im][column re/im] of the real 2 x 2 block
     const double v[4] = {a.x + b.x, b.y - a.y, a.y + b.y, a.x - b.x};
 #pragma unroll
-    for (int e = 0; e < 4; e++)
-      op[op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1))] = (float)v[e];
+    for (int e = 0; e < 4; e++) {
+      const int o = op_offset<S>(co, 2 * to + (e >> 1), 2 * ti + (e & 1));
+      const float x = (float)v[e], hi = tf32_round(x);
+      op[o] = hi;
+      op[S::OPS_FLOATS + o] = tf32_round(x - hi);
+    }
   }
 }
 
@@ -1500,7 +1507,7 @@ int tc_tree_prepare(tapas_b200_ctx *ctx) {
     T.iota_n = C;
   }
   if (T.tr_P != P) {
-    TB_CUDA(ctx, T.ops_tr.ensure((size_t)TcShape<P, true>::OPS_FLOATS * 8, s));
+    TB_CUDA(ctx, T.ops_tr.ensure((size_t)2 * TcShape<P, true>::OPS_FLOATS * 8, s));
     build_tree_ops<P><<<8, 256, 0, s>>>(ctx->cparent.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
                                         ctx->level_off[1], T.ops_tr.p);
     TB_LAUNCH_CHECK(ctx);
