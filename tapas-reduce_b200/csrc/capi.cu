@@ -213,6 +213,9 @@ int tapas_b200_ctx_destroy(tapas_b200_ctx *ctx) {
   ctx->p2p_counter.release();
   ctx->p2p_items.release();
   ctx->p2p_part.release();
+  for (auto *b : {&ctx->l2p_body_leaf}) b->release();
+  ctx->l2p_lf.release();
+  ctx->l2p_geo.release();
   ctx->tc.release();
   mlp_release(ctx);
   ctx->bh_attr.release();

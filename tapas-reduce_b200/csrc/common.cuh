@@ -184,6 +184,11 @@ struct tapas_b200_ctx {
   tb::DBuf<int2> trav_meta;            // traversal: per cell {nb, first child or -1 for a leaf}
   tb::DBuf<int32_t> flag, flag_scan;    // per-level scratch
   tb::DBuf<int32_t> leaf_list;          // indices of non-empty leaves
+  // mixed L2P, body-parallel: per evaluated leaf its FP32 local expansion and
+  // (centre, width); per body its leaf's ordinal (-1: not evaluated here)
+  tb::DBuf<float2> l2p_lf;
+  tb::DBuf<double4> l2p_geo;
+  tb::DBuf<int32_t> l2p_body_leaf;
   int64_t n_nonempty_leaves = 0;
   // Sharded evaluation (tapas_b200_set_owned_cells): per cell bit 0 = this
   // context computes the cell's local expansion, bit 1 = its bodies (P2M,

@@ -13,8 +13,8 @@
 //   L2P  - warp per non-empty leaf; lane per body, harmonics streamed in
 //          registers (no table), L of the leaf staged in shared memory.
 // Mixed form only: m2l_pair_kernel (the FP64 M2L of the pairs the tensor cores
-// leave, one warp per pair) and l2p32_kernel (L2P in FP32, in units of the
-// leaf width).
+// leave, one warp per pair) and l2p32_prep/l2p32_bodies (L2P in FP32, in units
+// of the leaf width, one thread per body).
 #include "expansions.cuh"
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
@@ -516,38 +516,55 @@ __global__ void __launch_bounds__(kThreads) l2p_kernel(
 // r' = r / w: every term L Y_n^m(r) is unchanged, the gradient is scaled by
 // 1/w at the end), which keeps every FP32 quantity bounded; L_n itself grows
 // like 1/R^(n+1) and leaves the FP32 range at high n in small cells.
+//
+// One thread per body: a warp per leaf would leave 23% of its lanes idle on a
+// surface tree (leaves of ~57 bodies take 2.3 passes of 32), so the leaves are
+// prepared first (l2p32_prep: the width-scaled FP32 local expansion and the
+// geometry, indexed by the leaf's ordinal, and each of its bodies' ordinal),
+// then l2p32_bodies evaluates every body, reading its leaf's coefficients
+// through L1 (the lanes of a warp share one to three leaves).
 template <int P>
-__global__ void __launch_bounds__(kThreads) l2p32_kernel(
+__global__ void __launch_bounds__(256) l2p32_prep(
     const int32_t *__restrict__ leaves, int64_t nleaves, const int32_t *__restrict__ cbeg,
     const int32_t *__restrict__ cnb, const double *__restrict__ ccen,
     const double *__restrict__ cmin, const double *__restrict__ cmax,
-    const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
-    const double *__restrict__ sq, const double2 *__restrict__ L, double *__restrict__ trg,
-    int near_has_q) {
+    const double2 *__restrict__ L, float2 *__restrict__ Lf, double4 *__restrict__ geo,
+    int32_t *__restrict__ body_leaf) {
   using S = Sizes<P>;
-  __shared__ float2 Lsm[kWarps][S::NT];
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-  const int64_t w = (int64_t)blockIdx.x * kWarps + wi;
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
   if (w >= nleaves) return;
   const int c = leaves[w];
-  const int b0 = cbeg[c], nb = cnb[c];
-  float2 *Lc = Lsm[wi];
-  const double width = cmax[3 * c] - cmin[3 * c], iw = 1.0 / width;
+  const double width = cmax[3 * c] - cmin[3 * c];
   for (int t = lane; t < S::NT; t += 32) {
     int n, m;
     jk_of(t, n, m);
     double wn = 1.0;
     for (int k = 0; k < n; k++) wn *= width;
     const double2 v = L[(int64_t)c * S::NT + t];
-    Lc[t] = make_float2((float)(v.x * wn), (float)(v.y * wn));
+    Lf[w * S::NT + t] = make_float2((float)(v.x * wn), (float)(v.y * wn));
   }
-  __syncwarp();
-  const double cx = ccen[3 * c], cy = ccen[3 * c + 1], cz = ccen[3 * c + 2];
-  for (int b = lane; b < nb; b += 32) {
-    const int64_t bi = b0 + b;
-    const float dx = (float)((sx[bi] - cx) * iw), dy = (float)((sy[bi] - cy) * iw),
-                dz = (float)((sz[bi] - cz) * iw);
-    // cart2sph (:43-47): r, cos/sin of theta and e^{i phi} from the offset
+  if (lane == 0) geo[w] = make_double4(ccen[3 * c], ccen[3 * c + 1], ccen[3 * c + 2], width);
+  const int b0 = cbeg[c], nb = cnb[c];
+  for (int b = lane; b < nb; b += 32) body_leaf[b0 + b] = (int32_t)w;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) l2p32_bodies(
+    int64_t n, const int32_t *__restrict__ body_leaf, const double4 *__restrict__ geo,
+    const float2 *__restrict__ Lf, const double *__restrict__ sx,
+    const double *__restrict__ sy, const double *__restrict__ sz,
+    const double *__restrict__ sq, double *__restrict__ trg, int near_has_q) {
+  using S = Sizes<P>;
+  for (int64_t bi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; bi < n;
+       bi += (int64_t)gridDim.x * blockDim.x) {
+    const int w = body_leaf[bi];
+    if (w < 0) continue;  // a body another context evaluates
+    const double4 g = geo[w];
+    const double iw = 1.0 / g.w;
+    const float2 *__restrict__ Lc = Lf + (int64_t)w * S::NT;
+    const float dx = (float)((sx[bi] - g.x) * iw), dy = (float)((sy[bi] - g.y) * iw),
+                dz = (float)((sz[bi] - g.z) * iw);
     const float rxy2 = dx * dx + dy * dy;
     const float r = sqrtf(rxy2 + dz * dz);
     float x = 1.f, y = 0.f, cp = 1.f, sp = 0.f;
@@ -566,36 +583,36 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
     float2 eim = make_float2(1.f, 0.f);
 #pragma unroll
     for (int m = 0; m < P; m++) {
-      // keeps the compiler from hoisting every column's shared-memory loads
-      // of L ahead of the loop (168 registers at P = 15 instead of 80)
+      // keeps the compiler from hoisting every column's loads of the
+      // coefficients ahead of the loop (register pressure)
       asm volatile("" ::: "memory");
       float p = pn, p1 = pn;
       float rhon = rhom;
       float2 sa = make_float2(0.f, 0.f), sb = sa, sc = sa;
 #pragma unroll
-      for (int n = m; n < P; n++) {
+      for (int nn = m; nn < P; nn++) {
         float ys, yt;
         const float t1 = x * p1;
-        if (n == m) {
+        if (nn == m) {
           const float pnew = (float)(2 * m + 1) * t1;
           ys = rhom * p;
           yt = rhom * (pnew - (float)(m + 1) * t1);
           p = pnew;
           rhon = rhom * r;
         } else {
-          rhon *= 1.f / (float)(-(n + m));  // constants after unrolling
+          rhon *= 1.f / (float)(-(nn + m));
           ys = rhon * p;
           const float p2 = p1;
           p1 = p;
           const float tn = x * p1;
-          p = ((float)(2 * n + 1) * tn - (float)(n + m) * p2) * (1.f / (float)(n - m + 1));
-          yt = rhon * ((float)(n - m + 1) * p - (float)(n + 1) * tn);
+          p = ((float)(2 * nn + 1) * tn - (float)(nn + m) * p2) * (1.f / (float)(nn - m + 1));
+          yt = rhon * ((float)(nn - m + 1) * p - (float)(nn + 1) * tn);
           rhon *= r;
         }
-        const float2 Lv = Lc[n * (n + 1) / 2 + m];
+        const float2 Lv = __ldg(Lc + nn * (nn + 1) / 2 + m);
         sa.x = fmaf(ys, Lv.x, sa.x);
         sa.y = fmaf(ys, Lv.y, sa.y);
-        const float nys = (float)n * ys;
+        const float nys = (float)nn * ys;
         sb.x = fmaf(nys, Lv.x, sb.x);
         sb.y = fmaf(nys, Lv.y, sb.y);
         sc.x = fmaf(yt, Lv.x, sc.x);
@@ -606,7 +623,7 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
       pot += f * zax;
       s0 += f * inv_r * (sb.x * eim.x - sb.y * eim.y);
       s1 += f * inv_y * (sc.x * eim.x - sc.y * eim.y);
-      if (m > 0) s2 += 2.f * (-zay) * (float)m;  // real(L*Y*i) = -imag(L*Y)
+      if (m > 0) s2 += 2.f * (-zay) * (float)m;
       rhom = rhom * r * (1.f / (float)(-(2 * m + 2) * (2 * m + 1)));
       pn = -pn * fact * y;
       fact += 2.f;
@@ -617,8 +634,6 @@ __global__ void __launch_bounds__(kThreads) l2p32_kernel(
     const float c1 = st * sp * s0 + ct * sp * inv_r * s1 + cp * inv_r * inv_y * s2;
     const float c2 = ct * s0 - st * inv_r * s1;
     double *o = trg + 4 * bi;
-    // an FP64 near field holds q_i * sum(q_j / r) (the reference's TRG before
-    // its `ba /= b.SRC`)
     const double iq = near_has_q ? 1.0 / sq[bi] : 1.0;
     o[0] = o[0] * iq + (double)pot;
     o[1] = o[1] * iq + (double)c0 * iw;
@@ -1388,11 +1403,18 @@ int downward_P(tapas_b200_ctx *ctx, bool l2p_f32) {
   int64_t nl = 0;
   const int32_t *leaves = work_leaves(ctx, nl);  // sharded: owned leaves only
   if (nl > 0 && l2p_f32) {
-    l2p32_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
-        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p,
-        ctx->sx.p, ctx->sy.p,
-        ctx->sz.p, ctx->sq.p, ctx->L.p, ctx->trg.p,
-        ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
+    TB_CUDA(ctx, ctx->l2p_lf.ensure((size_t)nl * Sizes<P>::NT, s));
+    TB_CUDA(ctx, ctx->l2p_geo.ensure((size_t)nl, s));
+    TB_CUDA(ctx, ctx->l2p_body_leaf.ensure((size_t)ctx->n, s));
+    if (ctx->sharded)  // bodies of other contexts' leaves: -1
+      TB_CUDA(ctx, cudaMemsetAsync(ctx->l2p_body_leaf.p, 0xff, sizeof(int32_t) * ctx->n, s));
+    l2p32_prep<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
+        leaves, nl, ctx->cbeg.p, ctx->cnb.p, ctx->ccen.p, ctx->cmin.p, ctx->cmax.p, ctx->L.p,
+        ctx->l2p_lf.p, ctx->l2p_geo.p, ctx->l2p_body_leaf.p);
+    TB_LAUNCH_CHECK(ctx);
+    l2p32_bodies<P><<<grid_for(ctx->n, kThreads, ctx->num_sms * 8), kThreads, 0, s>>>(
+        ctx->n, ctx->l2p_body_leaf.p, ctx->l2p_geo.p, ctx->l2p_lf.p, ctx->sx.p, ctx->sy.p,
+        ctx->sz.p, ctx->sq.p, ctx->trg.p, ctx->near_precision == TAPAS_B200_FP64 ? 1 : 0);
     TB_LAUNCH_CHECK(ctx);
   } else if (nl > 0) {
     l2p_kernel<P><<<(unsigned)((nl + kWarps - 1) / kWarps), kThreads, 0, s>>>(
