@@ -268,6 +268,23 @@ def test_deterministic(tb, ctx):
     assert _rel(a, b) < 1e-7
 
 
+def test_class_key_ranges_reused_and_renewed(tb, ctx):
+    """The M2L class keys are packed with the field ranges of the previous
+    classification; a list with larger offsets (smaller theta) misses them and
+    is classified again.  Either way the classes, and so the FP64 class-GEMM
+    result, equal a fresh context's bit for bit."""
+    x, y, z, q = tb.datasets.make("plummer", 60000, 41)
+    fresh = tb.Context(0)
+    try:
+        ref = {th: fresh.evaluate(x, y, z, q, P=8, ncrit=32, theta=th, precision=tb.FP64)
+               for th in (0.3, 0.6)}
+    finally:
+        fresh.close()
+    for th in (0.6, 0.3, 0.3, 0.6):
+        r = ctx.evaluate(x, y, z, q, P=8, ncrit=32, theta=th, precision=tb.FP64)
+        assert np.array_equal(r, ref[th])
+
+
 def test_mixed_traverse_lists_sorted_on_demand(tb, ctx):
     """The mixed form's traversal leaves each M2L target's sources unsorted
     (its M2L regroups the pairs by offset class); the list accessor and a
