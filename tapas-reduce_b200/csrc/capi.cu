@@ -338,7 +338,7 @@ int tapas_b200_get_device_view(tapas_b200_ctx *ctx, tapas_b200_device_view *out)
     set_error(ctx, "get_device_view: no tree (call partition first)");
     return TAPAS_B200_ERR_STATE;
   }
-  TB_TRY(sort_m2l_sources(ctx));  // the view's lists: sources in order per target
+  TB_TRY(sort_list_sources(ctx));  // the view's lists: sources in order per target
   *out = tapas_b200_device_view{};
   out->n_bodies = ctx->n;
   out->n_cells = ctx->ncells;
@@ -661,7 +661,7 @@ int tapas_b200_get_lists(tapas_b200_ctx *ctx, int32_t *m2l_tgt, int32_t *m2l_src
     set_error(ctx, "get_lists: no lists");
     return TAPAS_B200_ERR_STATE;
   }
-  TB_TRY(sort_m2l_sources(ctx));
+  TB_TRY(sort_list_sources(ctx));
   const int b = ctx->list_shift;
   const uint64_t mask = (1ull << b) - 1;
   for (int which = 0; which < 2; which++) {
@@ -693,7 +693,7 @@ int tapas_b200_m2l(tapas_b200_ctx *ctx, int precision) {
   if (precision == TAPAS_B200_MIXED) {
     TB_TRY(m2l_tensorcore(ctx));
   } else {
-    TB_TRY(sort_m2l_sources(ctx));  // the FP64 sums run in source order
+    TB_TRY(sort_list_sources(ctx, 0));  // the FP64 sums run in source order
     TB_TRY(m2l_fp64(ctx));
   }
   ctx->have_L = true;
@@ -710,14 +710,16 @@ int tapas_b200_p2p(tapas_b200_ctx *ctx, int precision) {
   PhaseTimer t(ctx, &ctx->timings.p2p);
   ctx->near_precision = precision;
   if (precision == TAPAS_B200_MIXED) return p2p_mixed(ctx);
+  TB_TRY(sort_list_sources(ctx, 1));  // the FP64 sums run in source order
   return p2p_fp64(ctx);
 }
 
 int tapas_b200_traverse(tapas_b200_ctx *ctx, double theta, int mutual, int precision) {
   TB_TRY(check_ctx(ctx));
   TB_TRY(check_precision(ctx, precision));
-  // the mixed M2L regroups its pairs by offset class: it needs the list
-  // grouped by target, not each target's sources sorted
+  // the mixed form needs the lists grouped by target, not each target's
+  // sources sorted (its M2L regroups the pairs by offset class, its FP32
+  // near field sums in any order)
   TB_TRY(build_lists(ctx, theta, mutual, precision != TAPAS_B200_MIXED));
   TB_TRY(tapas_b200_m2l(ctx, precision));
   return tapas_b200_p2p(ctx, precision);

@@ -200,8 +200,8 @@ struct tapas_b200_ctx {
 
   // ---- traversal lists ----
   bool have_lists = false;
-  bool m2l_sources_sorted = true;       // each M2L target's sources in increasing order
-  unsigned long long m2l_longest = 0;   // longest M2L target segment
+  bool sources_sorted[2] = {true, true};        // M2L, P2P: each target's sources in order
+  unsigned long long longest_segment[2] = {0, 0};  // M2L, P2P: longest target segment
   double theta = 0.4;
   tb::DBuf<int2> front_a, front_b;      // (target, source) pairs
   tb::DBuf<uint64_t> m2l, p2p;          // (target << 32 | source)

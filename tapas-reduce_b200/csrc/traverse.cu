@@ -423,23 +423,28 @@ int sort_segment_sources(tapas_b200_ctx *ctx, int w, unsigned long long longest)
 
 }  // namespace
 
-int sort_m2l_sources(tapas_b200_ctx *ctx) {
-  if (!ctx->have_lists || ctx->m2l_sources_sorted) return TAPAS_B200_OK;
-  const int64_t n = ctx->n_m2l;
+int sort_list_sources(tapas_b200_ctx *ctx, int w) {
+  if (!ctx->have_lists || ctx->sources_sorted[w]) return TAPAS_B200_OK;
+  const int64_t n = w ? ctx->n_p2p : ctx->n_m2l;
   if (n > 0) {
     cudaStream_t s = ctx->stream;
     TB_CUDA(ctx, ctx->list_src.ensure(n + 1, s));
     TB_CUDA(ctx, ctx->list_cnt.ensure(ctx->ncells + 1, s));
     list_sources<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
-        ctx->m2l.p, n, (1ull << ctx->list_shift) - 1, ctx->list_src.p);
+        w ? ctx->p2p.p : ctx->m2l.p, n, (1ull << ctx->list_shift) - 1, ctx->list_src.p);
     TB_LAUNCH_CHECK(ctx);
-    TB_TRY(sort_segment_sources(ctx, 0, ctx->m2l_longest));
+    TB_TRY(sort_segment_sources(ctx, w, ctx->longest_segment[w]));
   }
-  ctx->m2l_sources_sorted = true;
+  ctx->sources_sorted[w] = true;
   return TAPAS_B200_OK;
 }
 
-int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_m2l_sources) {
+int sort_list_sources(tapas_b200_ctx *ctx) {
+  TB_TRY(sort_list_sources(ctx, 0));
+  return sort_list_sources(ctx, 1);
+}
+
+int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_sources) {
   if (!ctx->have_tree) {
     set_error(ctx, "build_lists: no tree (call partition first)");
     return TAPAS_B200_ERR_STATE;
@@ -578,8 +583,10 @@ int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_m2l_sou
     TB_CUDA(ctx, cudaMemcpyAsync(hc + 5, ctx->counters.p + 5, 2 * sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, s));
     TB_CUDA(ctx, cudaStreamSynchronize(s));
-    ctx->m2l_longest = hc[5];
-    ctx->m2l_sources_sorted = true;
+    for (int w = 0; w < 2; w++) {
+      ctx->longest_segment[w] = hc[5 + w];
+      ctx->sources_sorted[w] = true;
+    }
     // 2. counting sort by target, then each target's sources
     for (int w = 0; w < 2; w++) {
       tb::DBuf<uint64_t> &L = *lists[w];
@@ -592,13 +599,13 @@ int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_m2l_sou
         scatter_by_target<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, s>>>(
             L.p, n, ctx->list_cnt.p, ctx->list_src.p);
         TB_LAUNCH_CHECK(ctx);
-        if (w == 0 && !sort_m2l_sources) {
-          // grouped by target only; sort_m2l_sources() completes the order
+        if (!sort_sources) {
+          // grouped by target only; sort_list_sources() completes the order
           // when a caller needs it
           pack_segments<<<grid_for(C, kSegWarps, ctx->num_sms * 8), kSegWarps * 32, 0, s>>>(
               ctx->list_src.p, offs[w]->p, C, b, L.p);
           TB_LAUNCH_CHECK(ctx);
-          ctx->m2l_sources_sorted = false;
+          ctx->sources_sorted[w] = false;
         } else {
           TB_TRY(sort_segment_sources(ctx, w, hc[5 + w]));
         }

@@ -5,10 +5,12 @@
 namespace tb {
 // mutual = 1: the reference's mutual traversal (every unordered cell pair
 // visited once); the lists are expanded to directed (target, source) pairs.
-// sort_m2l_sources = false (the mixed form, whose M2L regroups the pairs by
-// offset class): the M2L list is grouped by target, its sources not sorted
-// inside a target; sort_m2l_sources() sorts them where the order matters
-// (the FP64 M2L's summation order, the list and device-view accessors).
-int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_m2l_sources = true);
-int sort_m2l_sources(tapas_b200_ctx *ctx);
+// sort_sources = false (the mixed form): both lists are grouped by target,
+// each target's sources left in scatter order (the mixed M2L regroups its
+// pairs by offset class, and the FP32 near field sums in any order);
+// sort_list_sources() sorts them where the order matters (the FP64 M2L's and
+// P2P's summation order, the list and device-view accessors).
+int build_lists(tapas_b200_ctx *ctx, double theta, int mutual, bool sort_sources = true);
+int sort_list_sources(tapas_b200_ctx *ctx, int w);  // w = 0: M2L, 1: P2P
+int sort_list_sources(tapas_b200_ctx *ctx);         // both
 }  // namespace tb

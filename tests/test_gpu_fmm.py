@@ -286,10 +286,11 @@ def test_class_key_ranges_reused_and_renewed(tb, ctx):
 
 
 def test_mixed_traverse_lists_sorted_on_demand(tb, ctx):
-    """The mixed form's traversal leaves each M2L target's sources unsorted
-    (its M2L regroups the pairs by offset class); the list accessor and a
-    later FP64 M2L see them sorted, as build_lists gives them, so an FP64
-    evaluation after a mixed traversal equals a plain one bit for bit."""
+    """The mixed form's traversal leaves each target's sources unsorted in both
+    lists (its M2L regroups the pairs by offset class, its FP32 near field sums
+    in any order); the list accessor and a later FP64 M2L and P2P see them
+    sorted, as build_lists gives them, so an FP64 evaluation after a mixed
+    traversal equals a plain one bit for bit."""
     x, y, z, q = tb.datasets.make("sphere_surface", 40000, 3)
     fp64 = ctx.evaluate(x, y, z, q, P=6, ncrit=32, theta=0.4, precision=tb.FP64)
     (mt0, ms0), (pt0, ps0) = ctx.lists()
