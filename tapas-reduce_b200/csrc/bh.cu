@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(128) bh_walk_kernel(
     const float4 *__restrict__ attr32, const float4 *__restrict__ pos32, double theta,
     double eps2, double *__restrict__ out, unsigned long long *__restrict__ counters) {
   int stack[kStack];
+  const double theta2 = __dmul_rn(theta, theta);
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long napprox = 0, ndirect = 0, overflow = 0;
   if (b < n) {
@@ -133,9 +134,18 @@ __global__ void __launch_bounds__(128) bh_walk_kernel(
                    dz = __dsub_rn(pz, T.ccen[3 * c + 2]);
       double R = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
       R = __dadd_rn(R, __dmul_rn(dz, dz));
-      const double d = __dsqrt_rn(R);
       const double s = __dsub_rn(T.cmax[3 * c], T.cmin[3 * c]);
-      if (__ddiv_rn(s, d) < theta) {
+      // The sample evaluates fl(s / fl(sqrt(R))) < theta.  That value is
+      // s/sqrt(R) within ~2.3 ulp, and s^2 against theta^2 R below within
+      // ~4 ulp, so outside a relative band of 1e-13 around theta^2 R the
+      // squared test decides the same way without the square root and the
+      // division; inside it the sample's own operations decide.
+      const double s2 = __dmul_rn(s, s), t2R = __dmul_rn(theta2, R);
+      bool accept;
+      if (s2 < __dmul_rn(t2R, 1.0 - 1e-13)) accept = true;
+      else if (s2 > __dmul_rn(t2R, 1.0 + 1e-13)) accept = false;
+      else accept = __ddiv_rn(s, __dsqrt_rn(R)) < theta;
+      if (accept) {
         if (kFp64) {
           const double4 a = attr[c];
           force64(px, py, pz, a.x, a.y, a.z, a.w, eps2, o64);
