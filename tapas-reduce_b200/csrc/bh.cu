@@ -6,13 +6,14 @@
 //                   body, a non-leaf the mass and mass-weighted centre of its 8
 //                   children summed in index order (leaves with more bodies,
 //                   ncrit > 1, use the same formula over their bodies).
-//  bh_walk_kernel   interact + ComputeForce (bh.cc:135-153, 192-224): one
-//                   thread per body (bodies in Morton order, so a warp's walks
-//                   stay close) walks the tree depth first from the root with a
-//                   bounded explicit stack, children visited 0..7 like the
-//                   sample's recursion.  A cell is accepted when
-//                   width / |centre - body| < theta; a leaf is summed body by
-//                   body (the body itself included, as in the sample).
+//  bh_walk_kernel   interact + ComputeForce (bh.cc:135-153, 192-224): each
+//                   body walks the tree depth first from the root, children
+//                   visited 0..7 like the sample's recursion; a warp's 32
+//                   bodies (consecutive in Morton order) share one bounded
+//                   stack of the union of their walks (below).  A cell is
+//                   accepted when width / |centre - body| < theta; a leaf is
+//                   summed body by body (the body itself included, as in the
+//                   sample).
 // The FP64 form uses separately rounded operations in the sample's order, so
 // it reproduces the sample bit for bit; the FP32 form ("mixed") walks with FP32
 // positions and FP32 copies of the FP64 cell moments.
@@ -97,26 +98,51 @@ struct BhTree {
   const double *cmin, *cmax, *ccen;
 };
 
+// One walk per warp over the union of its 32 bodies' walks.  The warp keeps
+// one stack of (cell, lanes that reach it); at each popped cell the lanes in
+// its mask do what their own walk does there (sum a leaf, accept the cell, or
+// open it), and the cell's children are pushed for the lanes that opened it.
+// Every lane's walk is a depth-first walk with children 0..7 of a subtree of
+// the union's, so a lane meets its cells in its own order, takes the sample's
+// decisions and sums its interactions in the sample's order; the warp reads
+// each cell and each leaf body once for all its lanes, and the bodies, in
+// Morton order, share most of their walks.
+constexpr int kWalkWarps = 4;
 template <bool kFp64>
-__global__ void __launch_bounds__(128) bh_walk_kernel(
+__global__ void __launch_bounds__(32 * kWalkWarps) bh_walk_kernel(
     BhTree T, int64_t n, const double *__restrict__ sx, const double *__restrict__ sy,
     const double *__restrict__ sz, const double *__restrict__ sm, const double4 *__restrict__ attr,
     const float4 *__restrict__ attr32, const float4 *__restrict__ pos32, double theta,
     double eps2, double *__restrict__ out, unsigned long long *__restrict__ counters) {
-  int stack[kStack];
+  __shared__ int scell[kWalkWarps][kStack];
+  __shared__ unsigned smask[kWalkWarps][kStack];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const double theta2 = __dmul_rn(theta, theta);
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = b < n;
   unsigned long long napprox = 0, ndirect = 0, overflow = 0;
-  if (b < n) {
-    const double px = sx[b], py = sy[b], pz = sz[b];
-    double4 o64 = make_double4(0, 0, 0, 0);
-    float4 o32 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 p32 = kFp64 ? make_float4(0.f, 0.f, 0.f, 0.f) : pos32[b];
-    int sp = 0;
-    stack[sp++] = 0;
-    while (sp > 0) {
-      const int c = stack[--sp];
-      if (T.leaf[c]) {
+  const double px = valid ? sx[b] : 0.0, py = valid ? sy[b] : 0.0, pz = valid ? sz[b] : 0.0;
+  double4 o64 = make_double4(0, 0, 0, 0);
+  float4 o32 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 p32 = (kFp64 || !valid) ? make_float4(0.f, 0.f, 0.f, 0.f) : pos32[b];
+  const unsigned lanes = __ballot_sync(0xffffffffu, valid);
+  int sp = 0;  // the same in every lane
+  if (lanes) {
+    if (lane == 0) {
+      scell[wi][0] = 0;
+      smask[wi][0] = lanes;
+    }
+    sp = 1;
+    __syncwarp();
+  }
+  while (sp > 0) {
+    --sp;
+    const int c = scell[wi][sp];
+    const unsigned m = smask[wi][sp];
+    __syncwarp();  // read before a push reuses the slot
+    const bool mine = (m >> lane) & 1u;
+    if (T.leaf[c]) {
+      if (mine) {
         const int nb = T.nb[c], b0 = T.beg[c];
         for (int i = 0; i < nb; i++) {
           const int j = b0 + i;
@@ -127,8 +153,11 @@ __global__ void __launch_bounds__(128) bh_walk_kernel(
           }
         }
         ndirect += (unsigned)nb;
-        continue;
       }
+      continue;
+    }
+    bool open = false;
+    if (mine) {
       // the sample's MAC: cell width / |centre - body| < theta
       const double dx = __dsub_rn(px, T.ccen[3 * c]), dy = __dsub_rn(py, T.ccen[3 * c + 1]),
                    dz = __dsub_rn(pz, T.ccen[3 * c + 2]);
@@ -155,14 +184,25 @@ __global__ void __launch_bounds__(128) bh_walk_kernel(
         }
         napprox++;
       } else {
-        if (sp + 8 > kStack) {
-          overflow = 1;
-          break;
-        }
-        const int ch = T.child[c];
-        for (int i = 7; i >= 0; i--) stack[sp++] = ch + i;  // child 0 is visited first
+        open = true;
       }
     }
+    const unsigned om = __ballot_sync(0xffffffffu, open);
+    if (om) {
+      if (sp + 8 > kStack) {
+        if (mine) overflow = 1;
+        break;
+      }
+      // children 7..0 from the bottom up, so child 0 is popped first
+      if (lane < 8) {
+        scell[wi][sp + lane] = T.child[c] + 7 - lane;
+        smask[wi][sp + lane] = om;
+      }
+      sp += 8;
+      __syncwarp();
+    }
+  }
+  if (valid) {
     double4 *o = reinterpret_cast<double4 *>(out) + b;
     *o = kFp64 ? o64 : make_double4((double)o32.x, (double)o32.y, (double)o32.z, (double)o32.w);
   }
@@ -171,7 +211,7 @@ __global__ void __launch_bounds__(128) bh_walk_kernel(
     ndirect += __shfl_down_sync(0xffffffffu, ndirect, s);
     overflow |= __shfl_down_sync(0xffffffffu, overflow, s);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
     if (napprox) atomicAdd(counters + 0, napprox);
     if (ndirect) atomicAdd(counters + 1, ndirect);
     if (overflow) atomicOr(counters + 2, 1ull);
@@ -232,9 +272,9 @@ int bh_interact(tapas_b200_ctx *ctx, double theta, double eps2, int precision) {
   BhTree T{ctx->cleaf.p, ctx->cnb.p, ctx->cbeg.p, ctx->cchild.p, ctx->cmin.p, ctx->cmax.p,
            ctx->ccen.p};
   PhaseTimer t(ctx, &ctx->timings.p2p);
-  const int grid = (int)((n + 127) / 128);
+  const int grid = (int)((n + 32 * kWalkWarps - 1) / (32 * kWalkWarps));
   if (precision == TAPAS_B200_FP64) {
-    bh_walk_kernel<true><<<grid, 128, 0, s>>>(T, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p,
+    bh_walk_kernel<true><<<grid, 32 * kWalkWarps, 0, s>>>(T, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p,
                                               ctx->bh_attr.p, nullptr, nullptr, theta, eps2,
                                               ctx->trg.p, ctx->counters.p);
   } else {
@@ -244,7 +284,7 @@ int bh_interact(tapas_b200_ctx *ctx, double theta, double eps2, int precision) {
                                                      ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p,
                                                      ctx->rel4.p);
     TB_LAUNCH_CHECK(ctx);
-    bh_walk_kernel<false><<<grid, 128, 0, s>>>(T, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p,
+    bh_walk_kernel<false><<<grid, 32 * kWalkWarps, 0, s>>>(T, n, ctx->sx.p, ctx->sy.p, ctx->sz.p, ctx->sq.p,
                                                ctx->bh_attr.p, ctx->bh_attr32.p, ctx->rel4.p,
                                                theta, eps2, ctx->trg.p, ctx->counters.p);
   }
